@@ -1,0 +1,169 @@
+/*
+ * pigment_mpm.h -- C ABI of the B200 paint-mixing MPM step (drop-in for the reference's
+ * `Simulation` setup/step API, Natashaaak/pigment_mixing matter/src/simulation/simulation.hpp:25-186).
+ *
+ * One `pm_sim` is one `Simulation`.  All particle and grid state lives in GPU memory; host
+ * buffers passed to the calls below are copied in or out.  Every call returns a pm_status.
+ * Plain C types only: the library can be bound from C, C++, ctypes, cgo, JNI or N-API.
+ *
+ * Each declaration names the reference interface it replaces (file:line in the reference
+ * repository).  Enumerations keep the reference's numeric values (matter/src/tools.hpp:55-59).
+ */
+#ifndef PIGMENT_MPM_H
+#define PIGMENT_MPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define PM_API __declspec(dllexport)
+#else
+#define PM_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pm_sim pm_sim;
+
+typedef enum pm_status {
+  PM_OK = 0,
+  PM_ERR_INVALID = 1,      /* bad argument or unknown parameter name */
+  PM_ERR_STATE = 2,        /* call out of order (e.g. step before prepare) */
+  PM_ERR_CUDA = 3,         /* a CUDA call failed; pm_last_error_message() has the text */
+  PM_ERR_IO = 4,           /* a file could not be read */
+  PM_ERR_UNSUPPORTED = 5,  /* model or option not implemented on this path */
+  PM_ERR_CAPACITY = 6      /* a size limit was exceeded */
+} pm_status;
+
+/* matter/src/tools.hpp:55 */
+typedef enum pm_plate_type { PM_PLATE_TOP = 0, PM_PLATE_BOTTOM, PM_PLATE_LEFT, PM_PLATE_RIGHT, PM_PLATE_FRONT,
+                             PM_PLATE_BACK } pm_plate_type;
+/* matter/src/tools.hpp:59 */
+typedef enum pm_bc { PM_BC_NOSLIP = 0, PM_BC_SLIPSTICK = 1, PM_BC_SLIPFREE = 2 } pm_bc;
+/* matter/src/tools.hpp:57; this path implements NoPlasticity, VMVisc and DPVisc */
+typedef enum pm_plastic_model { PM_NO_PLASTICITY = 0, PM_VM = 1, PM_DP = 2, PM_DPSOFT = 3, PM_MCC = 4,
+                                PM_VMVISC = 5, PM_DPVISC = 6, PM_MCCVISC = 7, PM_DPMUI = 8,
+                                PM_MCCMUI = 9 } pm_plastic_model;
+/* Return-map implementation (no reference counterpart: the learned surrogate is new). */
+typedef enum pm_return_map { PM_RETURN_MAP_PLAIN = 0, PM_RETURN_MAP_SURROGATE = 1 } pm_return_map;
+
+/* Device error bits read by pm_get_error_flags (the reference's `int exit`, simulation.hpp:30). */
+#define PM_FLAG_NEG_DGAMMA 0x1u    /* plasticity.cpp:186-192, 286-289 */
+#define PM_FLAG_NEWTON_NOCONV 0x2u /* plasticity.cpp:200-203, 298-301 */
+#define PM_FLAG_NEWTON_FLAT 0x4u   /* plasticity.cpp:219-222, 314-317 */
+#define PM_FLAG_INVALID_BC 0x8u    /* boundary_collision.cpp:84-88 */
+#define PM_FLAG_NAN_PARTICLE 0x10u /* position_update.cpp:311-327: a particle was deactivated */
+#define PM_FLAG_INDEX_RANGE 0x20u  /* a particle fell outside the step's grid (never expected) */
+#define PM_FLAG_CAPACITY 0x40u     /* grid capacity exceeded; the host regrows and resumes */
+
+/* ---- lifetime ---------------------------------------------------------------------------- */
+/* Simulation::Simulation() (simulation.cpp:3-22).  device: CUDA ordinal. */
+PM_API pm_status pm_create(int device, pm_sim** out);
+/* ~Simulation() */
+PM_API pm_status pm_destroy(pm_sim* sim);
+/* Text of the last error on this thread (static storage, never NULL). */
+PM_API const char* pm_last_error_message(void);
+
+/* Simulation::initializeBasic(name) (simulation_units.cpp:9-26). */
+PM_API pm_status pm_initialize_basic(pm_sim* sim, const char* name);
+
+/* ---- parameters: the public fields of Simulation (simulation.hpp:38-126) ---------------- */
+/* Scalar fields by name: "cfl", "cfl_elastic", "flip_ratio", "rho", "E", "nu", "fps", "end_frame",
+ * "min_dt", "dx", "particle_mass", "particle_volume", "plastic_model", "use_pradhana", "use_musl",
+ * "use_particle_boundaries", "q_max", "q_min", "p_min", "M", "q_cohesion", "perzyna_exp",
+ * "perzyna_visc", "xi", "q_prefac", "pigment_D_max", "pigment_D_edge0", "pigment_D_edge1",
+ * "start_boost_time", "end_boost_time", "boost_factor", "frame", "auto_frame".
+ * Read-only extras for pm_get_param: "time", "dt", "step", "Np", "mu", "lambda", "K", "dt_max",
+ * "frame_dt", "final_time", "n_active", "plastic_count", "grid_nodes". */
+PM_API pm_status pm_set_param(pm_sim* sim, const char* name, double value);
+PM_API pm_status pm_get_param(pm_sim* sim, const char* name, double* value);
+/* Vector fields: "gravity", "particle_boundary_min", "particle_boundary_max", "grid_reference_point". */
+PM_API pm_status pm_set_param3(pm_sim* sim, const char* name, const double value[3]);
+
+/* The JSON readers of Simulation::setupScene (simulation_units.cpp:31-80): same keys, same
+ * defaults when a key is absent; a missing file leaves the fields as set (the reference's
+ * file-missing defaults are applied by pm_setup_scene).  Returns PM_ERR_IO on a parse error. */
+PM_API pm_status pm_load_pigment_config(pm_sim* sim, const char* path);
+PM_API pm_status pm_load_sim_config(pm_sim* sim, const char* path);
+
+/* ---- particles (Simulation::particles / Np, data_structures.hpp:9-50) --------------------- */
+/* Host arrays, row-major: x[n*3], latent[n*7] (Mixbox latent: 4 concentrations + 3 RGB
+ * residuals), v[n*3] or NULL for zero.  Resets F to identity and all plastic state to zero. */
+PM_API pm_status pm_set_particles(pm_sim* sim, uint32_t n, const float* x, const float* latent, const float* v);
+/* Copies particle state back to host arrays in the original particle order.  Any pointer may
+ * be NULL.  F and B: n*9 row-major; plastic: n*4 (eps_pl_dev, eps_pl_vol, eps_pl_vol_pradhana,
+ * delta_gamma); active: n bytes (0/1). */
+PM_API pm_status pm_get_particles(pm_sim* sim, float* x, float* v, float* latent, float* diffusion, uint8_t* active,
+                           float* F, float* B, float* plastic);
+
+/* ---- object plugins --------------------------------------------------------------------- */
+/* ObjectPlate(pos, type, bc, friction, pos_lower, pos_upper, vx, vy, vz, vmin_factor,
+ * load_factor) (object_plate.hpp:13-28). */
+PM_API pm_status pm_add_plate(pm_sim* sim, double pos, int plate_type, int bc, double friction, double pos_lower,
+                       double pos_upper, double vx, double vy, double vz, double vmin_factor, double load_factor);
+/* ObjectSpatula(bc, friction, name, anim_path) (object_spatula.hpp:16-37) with the keyframes
+ * given in memory: frames[n*7] = position xyz, quaternion xyzw at 60 frames/s. */
+PM_API pm_status pm_add_spatula(pm_sim* sim, int bc, double friction, const float* frames, uint32_t n);
+/* Same, reading a spatula_motion.bin file (ObjectSpatula::loadAnimation, object_spatula.hpp:235-250). */
+PM_API pm_status pm_add_spatula_file(pm_sim* sim, int bc, double friction, const char* anim_path);
+/* Box knife (no reference counterpart; the synthetic workloads' knife): a box SDF with the given
+ * half extents, fixed orientation quat_wxyz (NULL = identity), centre moving along the polyline
+ * waypoints[n*3] at `speed` units/s.  Like the spatula it is the scene's knife
+ * (spatula_ptr, simulation.hpp:131) and takes the knife-specific collision rules. */
+PM_API pm_status pm_add_box_knife(pm_sim* sim, int bc, double friction, const double half[3], const double* waypoints,
+                           uint32_t n, double speed, const double* quat_wxyz);
+/* ObjectGround(bc, friction, name, y) (object_ground.hpp:14) and ObjectCurve(bc, friction)
+ * (object_curve.hpp:13), the analytic colliders of the reference's tests. */
+PM_API pm_status pm_add_ground(pm_sim* sim, int bc, double friction, double y0);
+PM_API pm_status pm_add_curve(pm_sim* sim, int bc, double friction);
+
+/* ---- scene set-up and stepping ------------------------------------------------------------ */
+/* Simulation::setupScene(fps, colorRatios, pigments, anim_path) (simulation_units.cpp:28-131)
+ * without the OpenVDB blob sampling: the particles come from a prior pm_set_particles call.
+ * Reads the two JSON files (NULL = skip), sets gravity, particle boundaries [-2, 2]^3, the grid
+ * reference point (0,0,0), the bottom floor plate (SlipStick, friction 1), the spatula from
+ * anim_path (NULL = none), DPVisc with Pradhana correction and q_prefac = 1/sqrt(2). */
+PM_API pm_status pm_setup_scene(pm_sim* sim, float fps, const char* pigment_config_path, const char* sim_config_path,
+                         const char* anim_path);
+/* Simulation::prepareSimulation() (simulation_units.cpp:133-215): material constants, MUSL on,
+ * the initial grid (remeshFixedInit(2,2,2)), time = frame = 0.  Uploads objects. */
+PM_API pm_status pm_prepare(pm_sim* sim);
+/* Simulation::step() (simulation_units.cpp:217-233): one advanceStep, time += dt. */
+PM_API pm_status pm_step(pm_sim* sim);
+/* nsteps of { step(); frameFinished(); } -- the render loop's idiom (raytracing/src/main.cpp:
+ * 270-285) -- on the device without host round trips (CUDA graph replay).  *frames_done, if not
+ * NULL, receives the number of frame boundaries crossed. */
+PM_API pm_status pm_advance(pm_sim* sim, uint32_t nsteps, uint32_t* frames_done);
+/* Simulation::frameFinished() (simulation_units.cpp:235-241): mutates `frame`. */
+PM_API pm_status pm_frame_finished(pm_sim* sim, int* finished);
+/* Simulation::isFinished() (simulation_units.cpp:243-245). */
+PM_API pm_status pm_is_finished(pm_sim* sim, int* finished);
+/* Simulation::getGridBoundaries() (simulation_units.cpp:247-255). */
+PM_API pm_status pm_get_grid_boundaries(pm_sim* sim, double lo[3], double hi[3]);
+/* Simulation::getSpatulaObject() (simulation.hpp:186) as read by the renderer
+ * (MPMIntegrationSim.cpp:144-167): world->local transform (row-major 4x4) and the spatula's
+ * half width, half thickness, half length.  *exists = 0 when the scene has no knife. */
+PM_API pm_status pm_get_knife(pm_sim* sim, int* exists, double inv_transform[16], double half_dims[3]);
+/* Device error bits (PM_FLAG_*), accumulated since creation; clear = 1 resets them. */
+PM_API pm_status pm_get_error_flags(pm_sim* sim, uint32_t* flags, int clear);
+/* Conservation and mixing diagnostics over active particles (simulation.cpp:302-348,
+ * MPMIntegrationSim.cpp:48-90): total mass, momentum, mass-weighted mean latent. */
+PM_API pm_status pm_get_stats(pm_sim* sim, double* total_mass, double momentum[3], double mean_latent[7],
+                       uint32_t* n_active);
+/* Grid after the last step in lattice order (debug / parity): origin of node (0,0,0), dims, and
+ * per node mass, velocity after the grid update, MUSL velocity, flip, latent[7], shear.  Arrays
+ * have dims[0]*dims[1]*dims[2] entries; pass NULL arrays to query origin and dims only. */
+PM_API pm_status pm_get_grid(pm_sim* sim, double origin[3], uint32_t dims[3], float* mass, float* v_update,
+                      float* v_musl, float* flip, float* latent, float* shear);
+
+/* ---- learned return map (no reference counterpart) ----------------------------------------- */
+/* Selects the return-map implementation used by pm_step/pm_advance. */
+PM_API pm_status pm_set_return_map(pm_sim* sim, int mode);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIGMENT_MPM_H */

@@ -1,0 +1,1041 @@
+// Host runtime of the C ABI in include/pigment_mpm.h: owns device memory, the stream, the
+// CUDA graphs of the step, and the mirror of the reference Simulation's public fields.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/pigment_mpm.h"
+#include "pm_internal.cuh"
+#include "pm_launch.h"
+
+using namespace pm;
+
+namespace {
+
+thread_local std::string g_err;
+
+pm_status fail(pm_status s, const std::string& msg) {
+  g_err = msg;
+  return s;
+}
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return fail(PM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Public fields of Simulation with the reference's defaults (simulation.hpp:38-126).
+struct HostParams {
+  double fps = 1, cfl = 0.5, cfl_elastic = 1, flip_ratio = -0.95, rho = 1000, E = 1e5, nu = 0.3, min_dt = 1e-14;
+  double dx = 0, particle_mass = 0, particle_volume = 0;
+  double q_max = 100, q_min = 100, p_min = -1e20, M = 1, q_cohesion = 0, perzyna_exp = 1, perzyna_visc = 0, xi = 0;
+  double q_prefac = 1.0 / std::sqrt(2.0);
+  double D_max = 10e-2, D_edge0 = 0.5, D_edge1 = 0.8, start_boost = 20, end_boost = 40, boost_factor = 2;
+  double end_frame = 10;
+  int plastic_model = PM_NO_PLASTICITY;
+  int use_pradhana = 1, use_musl = 0, use_particle_boundaries = 0, auto_frame = 0;
+  double gravity[3] = {0, 0, 0};
+  double pbmin[3] = {-5, -5, -5}, pbmax[3] = {5, 5, 5};
+  double grid_ref[3] = {2e10, 2e10, 2e10};
+};
+
+// Minimal reader for a flat JSON object of numbers ({"key": number, ...}).
+bool parse_flat_json(const std::string& text, std::map<std::string, double>& out) {
+  size_t i = 0, n = text.size();
+  auto ws = [&]() { while (i < n && std::isspace((unsigned char)text[i])) ++i; };
+  ws();
+  if (i >= n || text[i] != '{') return false;
+  ++i;
+  ws();
+  if (i < n && text[i] == '}') return true;
+  while (i < n) {
+    ws();
+    if (i >= n || text[i] != '"') return false;
+    size_t j = text.find('"', i + 1);
+    if (j == std::string::npos) return false;
+    std::string key = text.substr(i + 1, j - i - 1);
+    i = j + 1;
+    ws();
+    if (i >= n || text[i] != ':') return false;
+    ++i;
+    ws();
+    const char* s = text.c_str() + i;
+    char* e = nullptr;
+    double v = std::strtod(s, &e);
+    if (e == s) {
+      if (text.compare(i, 4, "true") == 0) { v = 1; e = const_cast<char*>(s) + 4; }
+      else if (text.compare(i, 5, "false") == 0) { v = 0; e = const_cast<char*>(s) + 5; }
+      else return false;
+    }
+    i += (size_t)(e - s);
+    out[key] = v;
+    ws();
+    if (i < n && text[i] == ',') { ++i; continue; }
+    if (i < n && text[i] == '}') return true;
+    return false;
+  }
+  return false;
+}
+
+}  // namespace
+
+struct pm_sim {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string name;
+  HostParams hp;
+  std::vector<PlateDev> plates;
+  std::vector<ObjDev> objects;
+  int knife = -1;
+  std::vector<float> frames;
+  int return_map = PM_RETURN_MAP_PLAIN;
+
+  uint32_t np = 0;
+  int np_stride = 0;
+  float* d_pbuf[2] = {nullptr, nullptr};
+  uint32_t* d_meta[2] = {nullptr, nullptr};
+  int cur = 0;
+  float* d_pic = nullptr;
+  uint32_t *d_key = nullptr, *d_rank = nullptr, *d_sorted = nullptr;
+
+  int brick_cap = 0;
+  uint32_t* d_cell = nullptr;
+  uint32_t* d_scan_part = nullptr;
+  float4* d_grid = nullptr;
+  float4* d_gmusl = nullptr;
+
+  Ctrl* d_ctrl = nullptr;
+  Ctrl* h_ctrl = nullptr;  // pinned mirror
+  float* d_frames = nullptr;
+  float* d_unperm = nullptr;
+  uint8_t* d_active = nullptr;
+  double* d_stats = nullptr;
+  void* d_mlp = nullptr;
+
+  bool prepared = false;
+  uint32_t host_step = 0;  // steps completed (mirror of ctrl.step after the last sync)
+  Params P{};
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  bool graphs_dirty = true;
+
+  ~pm_sim();
+  void free_grid();
+  void free_particles();
+  pm_status alloc_grid(int bricks);
+  void fill_params();
+  Bufs bufs(int parity) const;
+  pm_status sync_ctrl();
+  pm_status push_ctrl();
+  pm_status run_steps(uint32_t n, bool use_graph);
+  pm_status capture_graphs();
+  void drop_graphs();
+};
+
+pm_sim::~pm_sim() {
+  drop_graphs();
+  free_particles();
+  free_grid();
+  if (d_ctrl) cudaFree(d_ctrl);
+  if (h_ctrl) cudaFreeHost(h_ctrl);
+  if (d_frames) cudaFree(d_frames);
+  if (d_stats) cudaFree(d_stats);
+  if (d_mlp) cudaFree(d_mlp);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void pm_sim::drop_graphs() {
+  for (int k = 0; k < 2; ++k)
+    if (gexec[k]) { cudaGraphExecDestroy(gexec[k]); gexec[k] = nullptr; }
+  graphs_dirty = true;
+}
+
+void pm_sim::free_grid() {
+  if (d_cell) cudaFree(d_cell);
+  if (d_scan_part) cudaFree(d_scan_part);
+  if (d_grid) cudaFree(d_grid);
+  if (d_gmusl) cudaFree(d_gmusl);
+  d_cell = nullptr; d_scan_part = nullptr; d_grid = nullptr; d_gmusl = nullptr;
+  brick_cap = 0;
+}
+
+void pm_sim::free_particles() {
+  for (int k = 0; k < 2; ++k) {
+    if (d_pbuf[k]) cudaFree(d_pbuf[k]);
+    if (d_meta[k]) cudaFree(d_meta[k]);
+    d_pbuf[k] = nullptr; d_meta[k] = nullptr;
+  }
+  if (d_pic) cudaFree(d_pic);
+  if (d_key) cudaFree(d_key);
+  if (d_rank) cudaFree(d_rank);
+  if (d_sorted) cudaFree(d_sorted);
+  if (d_unperm) cudaFree(d_unperm);
+  if (d_active) cudaFree(d_active);
+  d_pic = nullptr; d_key = d_rank = d_sorted = nullptr; d_unperm = nullptr; d_active = nullptr;
+}
+
+pm_status pm_sim::alloc_grid(int bricks) {
+  drop_graphs();
+  free_grid();
+  const size_t nodes = (size_t)bricks * kBrickNodes;
+  if (nodes + 2 > 0x7fffffffULL) return fail(PM_ERR_CAPACITY, "grid capacity exceeds 2^31 nodes");
+  CK(cudaMalloc(&d_cell, (nodes + 2) * sizeof(uint32_t)));
+  const size_t scan_blocks = (nodes + 1 + 4095) / 4096 + 1;
+  CK(cudaMalloc(&d_scan_part, scan_blocks * sizeof(uint32_t)));
+  CK(cudaMalloc(&d_grid, nodes * 4 * sizeof(float4)));
+  CK(cudaMalloc(&d_gmusl, nodes * sizeof(float4)));
+  CK(cudaMemsetAsync(d_grid, 0, nodes * 4 * sizeof(float4), stream));
+  CK(cudaMemsetAsync(d_gmusl, 0, nodes * sizeof(float4), stream));
+  brick_cap = bricks;
+  return PM_OK;
+}
+
+Bufs pm_sim::bufs(int parity) const {
+  Bufs b{};
+  b.pin = d_pbuf[parity];
+  b.pout = d_pbuf[parity ^ 1];
+  b.meta_in = d_meta[parity];
+  b.meta_out = d_meta[parity ^ 1];
+  b.pic = d_pic;
+  b.key = d_key;
+  b.rank = d_rank;
+  b.sorted = d_sorted;
+  b.cell = d_cell;
+  b.scan_part = d_scan_part;
+  b.grid = d_grid;
+  b.gmusl = d_gmusl;
+  b.ctrl = d_ctrl;
+  b.mlp = d_mlp;
+  return b;
+}
+
+void pm_sim::fill_params() {
+  Params& p = P;
+  const HostParams& h = hp;
+  p.np = (int)np;
+  p.np_stride = np_stride;
+  p.dx = (float)h.dx;
+  p.inv_dx = (float)(1.0 / h.dx);
+  p.dx_d = h.dx;
+  for (int d = 0; d < 3; ++d) {
+    p.anchor_d[d] = h_ctrl->low_init[d];
+    p.anchor[d] = (float)h_ctrl->low_init[d];
+    p.gravity[d] = (float)h.gravity[d];
+    p.pbmin[d] = (float)h.pbmin[d];
+    p.pbmax[d] = (float)h.pbmax[d];
+  }
+  p.particle_mass = (float)h.particle_mass;
+  p.particle_volume = (float)h.particle_volume;
+  p.apicD = (float)(4.0 / (h.dx * h.dx));
+  p.flip_ratio = (float)h.flip_ratio;
+  p.use_musl = h.use_musl;
+  p.use_particle_boundaries = h.use_particle_boundaries;
+  // simulation_units.cpp:167-183
+  p.lambda = h.nu * h.E / ((1.0 + h.nu) * (1.0 - 2.0 * h.nu));
+  p.mu = h.E / (2.0 * (1.0 + h.nu));
+  p.K = p.lambda + 2.0 * p.mu / 3.0;
+  p.d_prefac = 1.0 / h.q_prefac;
+  p.e_mu_prefac = 2.0 * h.q_prefac * p.mu;
+  p.f_mu_prefac = 2.0 * h.q_prefac * h.q_prefac * p.mu;
+  p.q_max = h.q_max; p.q_min = h.q_min; p.p_min = h.p_min; p.M = h.M; p.q_cohesion = h.q_cohesion;
+  p.perzyna_exp = h.perzyna_exp; p.perzyna_visc = h.perzyna_visc; p.xi = h.xi;
+  p.plastic_model = h.plastic_model;
+  p.use_pradhana = h.use_pradhana;
+  p.D_max = (float)h.D_max; p.D_edge0 = (float)h.D_edge0; p.D_edge1 = (float)h.D_edge1;
+  p.start_boost = (float)h.start_boost; p.end_boost = (float)h.end_boost; p.boost_factor = (float)h.boost_factor;
+  p.cfl = h.cfl;
+  const double wave_speed = std::sqrt(h.E / h.rho);
+  p.dt_max = h.cfl_elastic * h.dx / wave_speed;
+  p.frame_dt = 1.0 / h.fps;
+  p.min_dt = h.min_dt;
+  p.final_time = h.end_frame * p.frame_dt;
+  p.brick_cap = brick_cap;
+  p.node_cap = brick_cap * kBrickNodes;
+  p.frames = d_frames;
+  p.n_frames = (int)(frames.size() / 7);
+  p.return_map = return_map;
+  graphs_dirty = true;
+}
+
+pm_status pm_sim::sync_ctrl() {
+  CK(cudaMemcpyAsync(h_ctrl, d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  return PM_OK;
+}
+pm_status pm_sim::push_ctrl() {
+  CK(cudaMemcpyAsync(d_ctrl, h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  return PM_OK;
+}
+
+pm_status pm_sim::capture_graphs() {
+  drop_graphs();
+  for (int start = 0; start < 2; ++start) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    launch_step(P, bufs(start), stream);
+    launch_step(P, bufs(start ^ 1), stream);
+    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&gexec[start], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  graphs_dirty = false;
+  return PM_OK;
+}
+
+// Runs n steps; recovers from grid-capacity halts by regrowing and resuming.
+pm_status pm_sim::run_steps(uint32_t n, bool use_graph) {
+  uint32_t remaining = n;
+  int guard = 0;
+  while (remaining > 0) {
+    const uint32_t before = host_step;
+    uint32_t k = 0;
+    if (use_graph && remaining >= 2) {
+      if (graphs_dirty) { pm_status s = capture_graphs(); if (s != PM_OK) return s; }
+      int par = cur;
+      for (; k + 2 <= remaining; k += 2) CK(cudaGraphLaunch(gexec[par], stream));
+    }
+    int par = (cur + (int)k) & 1;
+    for (; k < remaining; ++k) { launch_step(P, bufs(par), stream); par ^= 1; }
+    CK(cudaGetLastError());
+    pm_status s = sync_ctrl();
+    if (s != PM_OK) return s;
+    const uint32_t done = h_ctrl->step - before;
+    host_step = h_ctrl->step;
+    cur = (cur + (int)done) & 1;
+    remaining -= std::min(done, remaining);
+    if (h_ctrl->halt) {
+      if (++guard > 8) return fail(PM_ERR_CAPACITY, "grid keeps overflowing after regrowth");
+      const int need = (int)h_ctrl->need_bricks;
+      const long long want = (long long)need * 3 / 2 + 64;
+      if (want * kBrickNodes > 0x7ffffff0LL) return fail(PM_ERR_CAPACITY, "grid would exceed 2^31 nodes");
+      s = alloc_grid((int)want);
+      if (s != PM_OK) return s;
+      fill_params();
+      h_ctrl->halt = 0;
+      h_ctrl->error_flags &= ~(uint32_t)E_CAPACITY;
+      s = push_ctrl();
+      if (s != PM_OK) return s;
+    }
+  }
+  return PM_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------
+extern "C" {
+
+const char* pm_last_error_message(void) { return g_err.c_str(); }
+
+pm_status pm_create(int device, pm_sim** out) {
+  if (!out) return fail(PM_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return fail(PM_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (device < 0 || device >= count) return fail(PM_ERR_INVALID, "device ordinal out of range");
+  CK(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) return fail(PM_ERR_UNSUPPORTED, "this library is built for sm_100a (B200) only");
+  pm_sim* s = new pm_sim();
+  s->device = device;
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) { delete s; return fail(PM_ERR_CUDA, "stream"); }
+  if (cudaMalloc(&s->d_ctrl, sizeof(Ctrl)) != cudaSuccess || cudaMallocHost(&s->h_ctrl, sizeof(Ctrl)) != cudaSuccess ||
+      cudaMalloc(&s->d_stats, 16 * sizeof(double)) != cudaSuccess) {
+    delete s;
+    return fail(PM_ERR_CUDA, "allocation of the control block failed");
+  }
+  std::memset(s->h_ctrl, 0, sizeof(Ctrl));
+  s->h_ctrl->knife = -1;
+  e = launch_init(device);
+  if (e != cudaSuccess) { delete s; return fail(PM_ERR_CUDA, std::string("kernel set-up: ") + cudaGetErrorString(e)); }
+  *out = s;
+  return PM_OK;
+}
+
+pm_status pm_destroy(pm_sim* sim) {
+  if (!sim) return PM_OK;
+  cudaSetDevice(sim->device);
+  if (sim->stream) cudaStreamSynchronize(sim->stream);
+  delete sim;
+  return PM_OK;
+}
+
+pm_status pm_initialize_basic(pm_sim* sim, const char* name) {
+  if (!sim) return fail(PM_ERR_INVALID, "sim is NULL");
+  sim->name = name ? name : "";
+  return PM_OK;
+}
+
+pm_status pm_set_param(pm_sim* sim, const char* name, double v) {
+  if (!sim || !name) return fail(PM_ERR_INVALID, "NULL argument");
+  HostParams& h = sim->hp;
+  std::string k(name);
+  bool ctrl_field = false;
+  if (k == "fps") h.fps = v;
+  else if (k == "cfl") h.cfl = v;
+  else if (k == "cfl_elastic") h.cfl_elastic = v;
+  else if (k == "flip_ratio") h.flip_ratio = v;
+  else if (k == "rho") h.rho = v;
+  else if (k == "E") h.E = v;
+  else if (k == "nu") h.nu = v;
+  else if (k == "min_dt") h.min_dt = v;
+  else if (k == "dx") h.dx = v;
+  else if (k == "particle_mass") h.particle_mass = v;
+  else if (k == "particle_volume") h.particle_volume = v;
+  else if (k == "q_max") h.q_max = v;
+  else if (k == "q_min") h.q_min = v;
+  else if (k == "p_min") h.p_min = v;
+  else if (k == "M") h.M = v;
+  else if (k == "q_cohesion") h.q_cohesion = v;
+  else if (k == "perzyna_exp") h.perzyna_exp = v;
+  else if (k == "perzyna_visc") h.perzyna_visc = v;
+  else if (k == "xi") h.xi = v;
+  else if (k == "q_prefac") h.q_prefac = v;
+  else if (k == "pigment_D_max") h.D_max = v;
+  else if (k == "pigment_D_edge0") h.D_edge0 = v;
+  else if (k == "pigment_D_edge1") h.D_edge1 = v;
+  else if (k == "start_boost_time") h.start_boost = v;
+  else if (k == "end_boost_time") h.end_boost = v;
+  else if (k == "boost_factor") h.boost_factor = v;
+  else if (k == "use_pradhana") h.use_pradhana = v != 0;
+  else if (k == "use_musl") h.use_musl = v != 0;
+  else if (k == "use_particle_boundaries") h.use_particle_boundaries = v != 0;
+  else if (k == "plastic_model") {
+    int m = (int)v;
+    if (m != PM_NO_PLASTICITY && m != PM_VMVISC && m != PM_DPVISC)
+      return fail(PM_ERR_UNSUPPORTED, "plastic_model: this path implements NoPlasticity, VMVisc and DPVisc");
+    h.plastic_model = m;
+  } else if (k == "end_frame") { h.end_frame = v; ctrl_field = true; }
+  else if (k == "frame") { ctrl_field = true; }
+  else if (k == "auto_frame") { h.auto_frame = v != 0; ctrl_field = true; }
+  else return fail(PM_ERR_INVALID, "unknown parameter " + k);
+  if (sim->prepared) {
+    if (k == "dx") return fail(PM_ERR_STATE, "dx cannot change after prepare");
+    if (ctrl_field) {
+      pm_status s = sim->sync_ctrl();
+      if (s != PM_OK) return s;
+      if (k == "frame") sim->h_ctrl->frame = (uint32_t)v;
+      if (k == "end_frame") sim->h_ctrl->end_frame = (uint32_t)v;
+      if (k == "auto_frame") sim->h_ctrl->auto_frame = (uint32_t)(v != 0);
+      s = sim->push_ctrl();
+      if (s != PM_OK) return s;
+    }
+    sim->fill_params();
+  }
+  return PM_OK;
+}
+
+pm_status pm_get_param(pm_sim* sim, const char* name, double* out) {
+  if (!sim || !name || !out) return fail(PM_ERR_INVALID, "NULL argument");
+  const HostParams& h = sim->hp;
+  std::string k(name);
+  if (sim->prepared && (k == "time" || k == "dt" || k == "step" || k == "frame" || k == "n_active" ||
+                        k == "plastic_count" || k == "grid_nodes")) {
+    pm_status s = sim->sync_ctrl();
+    if (s != PM_OK) return s;
+  }
+  const Ctrl* c = sim->h_ctrl;
+  if (k == "time") *out = c->time;
+  else if (k == "dt") *out = c->dt;
+  else if (k == "step") *out = c->step;
+  else if (k == "frame") *out = c->frame;
+  else if (k == "n_active") *out = c->n_active;
+  else if (k == "plastic_count") *out = c->plastic_count;
+  else if (k == "grid_nodes") *out = c->n_nodes;
+  else if (k == "Np") *out = sim->np;
+  else if (k == "fps") *out = h.fps;
+  else if (k == "cfl") *out = h.cfl;
+  else if (k == "cfl_elastic") *out = h.cfl_elastic;
+  else if (k == "flip_ratio") *out = h.flip_ratio;
+  else if (k == "rho") *out = h.rho;
+  else if (k == "E") *out = h.E;
+  else if (k == "nu") *out = h.nu;
+  else if (k == "dx") *out = h.dx;
+  else if (k == "particle_mass") *out = h.particle_mass;
+  else if (k == "particle_volume") *out = h.particle_volume;
+  else if (k == "M") *out = h.M;
+  else if (k == "q_cohesion") *out = h.q_cohesion;
+  else if (k == "perzyna_exp") *out = h.perzyna_exp;
+  else if (k == "perzyna_visc") *out = h.perzyna_visc;
+  else if (k == "q_max") *out = h.q_max;
+  else if (k == "q_min") *out = h.q_min;
+  else if (k == "q_prefac") *out = h.q_prefac;
+  else if (k == "plastic_model") *out = h.plastic_model;
+  else if (k == "use_musl") *out = h.use_musl;
+  else if (k == "use_pradhana") *out = h.use_pradhana;
+  else if (k == "end_frame") *out = h.end_frame;
+  else if (k == "pigment_D_max") *out = h.D_max;
+  else if (k == "pigment_D_edge0") *out = h.D_edge0;
+  else if (k == "pigment_D_edge1") *out = h.D_edge1;
+  else if (k == "start_boost_time") *out = h.start_boost;
+  else if (k == "end_boost_time") *out = h.end_boost;
+  else if (k == "boost_factor") *out = h.boost_factor;
+  else if (k == "mu") *out = sim->P.mu;
+  else if (k == "lambda") *out = sim->P.lambda;
+  else if (k == "K") *out = sim->P.K;
+  else if (k == "dt_max") *out = sim->P.dt_max;
+  else if (k == "frame_dt") *out = sim->P.frame_dt;
+  else if (k == "final_time") *out = sim->P.final_time;
+  else return fail(PM_ERR_INVALID, "unknown parameter " + k);
+  return PM_OK;
+}
+
+pm_status pm_set_param3(pm_sim* sim, const char* name, const double v[3]) {
+  if (!sim || !name || !v) return fail(PM_ERR_INVALID, "NULL argument");
+  std::string k(name);
+  double* dst = nullptr;
+  if (k == "gravity") dst = sim->hp.gravity;
+  else if (k == "particle_boundary_min") dst = sim->hp.pbmin;
+  else if (k == "particle_boundary_max") dst = sim->hp.pbmax;
+  else if (k == "grid_reference_point") dst = sim->hp.grid_ref;
+  else return fail(PM_ERR_INVALID, "unknown vector parameter " + k);
+  for (int d = 0; d < 3; ++d) dst[d] = v[d];
+  if (sim->prepared) sim->fill_params();
+  return PM_OK;
+}
+
+static std::string read_file(const char* path, bool& ok) {
+  std::ifstream f(path, std::ios::binary);
+  ok = (bool)f;
+  if (!ok) return std::string();
+  std::stringstream ss;
+  ss << f.rdbuf();
+  return ss.str();
+}
+
+pm_status pm_load_pigment_config(pm_sim* sim, const char* path) {
+  if (!sim || !path) return fail(PM_ERR_INVALID, "NULL argument");
+  bool ok = false;
+  std::string t = read_file(path, ok);
+  if (!ok) return PM_OK;  // simulation_units.cpp:46-48: keep current values
+  std::map<std::string, double> kv;
+  if (!parse_flat_json(t, kv)) return fail(PM_ERR_IO, std::string("parse error in ") + path);
+  auto get = [&](const char* key, double def) { auto it = kv.find(key); return it == kv.end() ? def : it->second; };
+  HostParams& h = sim->hp;  // simulation_units.cpp:36-41
+  h.D_max = get("D_max", 10e-2);
+  h.D_edge0 = get("D_edge0", 0.5);
+  h.D_edge1 = get("D_edge1", 0.8);
+  h.start_boost = get("start_boost_time", 20.0);
+  h.end_boost = get("end_boost_time", 40.0);
+  h.boost_factor = get("boost_factor", 2.0);
+  if (sim->prepared) sim->fill_params();
+  return PM_OK;
+}
+
+static void sim_config_file_missing_defaults(HostParams& h) {  // simulation_units.cpp:69-80
+  h.cfl = 0.2; h.flip_ratio = -0.8; h.E = 5e5; h.nu = 0.3; h.rho = 1000;
+  h.M = std::tan(5.0 * M_PI / 180.0); h.q_cohesion = 500; h.perzyna_exp = 1.0; h.perzyna_visc = 0.1;
+}
+
+pm_status pm_load_sim_config(pm_sim* sim, const char* path) {
+  if (!sim || !path) return fail(PM_ERR_INVALID, "NULL argument");
+  bool ok = false;
+  std::string t = read_file(path, ok);
+  if (!ok) { sim_config_file_missing_defaults(sim->hp); return PM_OK; }
+  std::map<std::string, double> kv;
+  if (!parse_flat_json(t, kv)) return fail(PM_ERR_IO, std::string("parse error in ") + path);
+  auto get = [&](const char* key, double def) { auto it = kv.find(key); return it == kv.end() ? def : it->second; };
+  HostParams& h = sim->hp;  // simulation_units.cpp:55-64
+  h.cfl = get("cfl", 0.2);
+  h.flip_ratio = get("flip_ratio", -0.8);
+  h.E = get("E", 500000.0);
+  h.nu = get("nu", 0.3);
+  h.rho = get("rho", 1000.0);
+  h.M = std::tan(get("friction_angle", 5.0) * M_PI / 180.0);
+  h.q_cohesion = get("q_cohesion", 500.0);
+  h.perzyna_exp = get("perzyna_exp", 1.0);
+  h.perzyna_visc = get("perzyna_visc", 0.1);
+  if (sim->prepared) sim->fill_params();
+  return PM_OK;
+}
+
+pm_status pm_set_particles(pm_sim* sim, uint32_t n, const float* x, const float* latent, const float* v) {
+  if (!sim || (n > 0 && !x)) return fail(PM_ERR_INVALID, "NULL argument");
+  if (n >= 0x7fffffffu) return fail(PM_ERR_CAPACITY, "too many particles");
+  cudaSetDevice(sim->device);
+  sim->drop_graphs();
+  sim->free_particles();
+  sim->np = n;
+  sim->np_stride = (int)((n + 31) / 32 * 32);
+  const size_t S = (size_t)std::max(sim->np_stride, 32);
+  for (int k = 0; k < 2; ++k) {
+    CK(cudaMalloc(&sim->d_pbuf[k], S * F_COUNT * sizeof(float)));
+    CK(cudaMalloc(&sim->d_meta[k], S * sizeof(uint32_t)));
+  }
+  CK(cudaMalloc(&sim->d_pic, S * 6 * sizeof(float)));
+  CK(cudaMalloc(&sim->d_key, S * sizeof(uint32_t)));
+  CK(cudaMalloc(&sim->d_rank, S * sizeof(uint32_t)));
+  CK(cudaMalloc(&sim->d_sorted, S * sizeof(uint32_t)));
+  CK(cudaMalloc(&sim->d_unperm, (size_t)std::max(n, 1u) * F_COUNT * sizeof(float)));
+  CK(cudaMalloc(&sim->d_active, std::max(n, 1u)));
+  std::vector<float> h(S * F_COUNT, 0.f);
+  std::vector<uint32_t> meta(S, 0);
+  for (uint32_t p = 0; p < n; ++p) {
+    for (int d = 0; d < 3; ++d) {
+      h[(F_X + d) * S + p] = x[3 * p + d];
+      h[(F_V + d) * S + p] = v ? v[3 * p + d] : 0.f;
+    }
+    h[(F_F + 0) * S + p] = 1.f; h[(F_F + 4) * S + p] = 1.f; h[(F_F + 8) * S + p] = 1.f;
+    if (latent) for (int k = 0; k < 7; ++k) h[(F_LAT + k) * S + p] = latent[7 * p + k];
+    meta[p] = p;
+  }
+  CK(cudaMemcpyAsync(sim->d_pbuf[0], h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
+  CK(cudaMemcpyAsync(sim->d_meta[0], meta.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, sim->stream));
+  CK(cudaStreamSynchronize(sim->stream));
+  sim->cur = 0;
+  sim->prepared = false;
+  sim->host_step = 0;
+  std::memset(sim->h_ctrl, 0, sizeof(Ctrl));
+  sim->h_ctrl->knife = -1;
+  return PM_OK;
+}
+
+pm_status pm_get_particles(pm_sim* sim, float* x, float* v, float* latent, float* diffusion, uint8_t* active, float* F,
+                           float* Bm, float* plastic) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  const uint32_t n = sim->np;
+  if (n == 0) return PM_OK;
+  CK(cudaSetDevice(sim->device));
+  Params p = sim->P;
+  p.np = (int)n;
+  p.np_stride = sim->np_stride;
+  launch_unpermute(p, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], sim->d_unperm, sim->d_active, sim->stream);
+  CK(cudaGetLastError());
+  std::vector<float> tmp;
+  auto fetch = [&](int f0, int nf, float* dst) -> pm_status {
+    if (!dst) return PM_OK;
+    tmp.resize((size_t)n * nf);
+    CK(cudaMemcpyAsync(tmp.data(), sim->d_unperm + (size_t)f0 * n, (size_t)n * nf * sizeof(float), cudaMemcpyDeviceToHost,
+                       sim->stream));
+    CK(cudaStreamSynchronize(sim->stream));
+    for (uint32_t q = 0; q < n; ++q)
+      for (int k = 0; k < nf; ++k) dst[(size_t)q * nf + k] = tmp[(size_t)k * n + q];
+    return PM_OK;
+  };
+  pm_status s;
+  if ((s = fetch(F_X, 3, x)) != PM_OK) return s;
+  if ((s = fetch(F_V, 3, v)) != PM_OK) return s;
+  if ((s = fetch(F_LAT, 7, latent)) != PM_OK) return s;
+  if ((s = fetch(F_DIFF, 1, diffusion)) != PM_OK) return s;
+  if ((s = fetch(F_F, 9, F)) != PM_OK) return s;
+  if ((s = fetch(F_B, 9, Bm)) != PM_OK) return s;
+  if ((s = fetch(F_EPD, 4, plastic)) != PM_OK) return s;
+  if (active) {
+    CK(cudaMemcpyAsync(active, sim->d_active, n, cudaMemcpyDeviceToHost, sim->stream));
+    CK(cudaStreamSynchronize(sim->stream));
+  }
+  return PM_OK;
+}
+
+pm_status pm_add_plate(pm_sim* sim, double pos, int plate_type, int bc, double friction, double pos_lower,
+                       double pos_upper, double vx, double vy, double vz, double vmin_factor, double load_factor) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (plate_type < 0 || plate_type > 5) return fail(PM_ERR_INVALID, "plate_type");
+  if (bc < 0 || bc > 2) return fail(PM_ERR_INVALID, "bc");
+  if ((int)sim->plates.size() >= kMaxPlates) return fail(PM_ERR_CAPACITY, "too many plates");
+  PlateDev p{};
+  p.type = plate_type; p.bc = bc; p.friction = (float)friction;
+  p.pos = pos; p.lower = pos_lower; p.upper = pos_upper;
+  p.vx = p.vx0 = (float)vx; p.vy = p.vy0 = (float)vy; p.vz = p.vz0 = (float)vz;
+  p.vmin_factor = (float)vmin_factor; p.load_factor = (float)load_factor;
+  sim->plates.push_back(p);
+  sim->prepared = false;
+  return PM_OK;
+}
+
+static void pose_from(ObjDev& o, const double t[3], const double q[4]) {
+  double n = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  double w = q[0] / n, x = q[1] / n, y = q[2] / n, z = q[3] / n;
+  double R[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w),
+                 2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
+                 2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)};
+  double det = R[0] * (R[4] * R[8] - R[5] * R[7]) - R[1] * (R[3] * R[8] - R[5] * R[6]) + R[2] * (R[3] * R[7] - R[4] * R[6]);
+  double inv[9] = {(R[4] * R[8] - R[5] * R[7]) / det, (R[2] * R[7] - R[1] * R[8]) / det, (R[1] * R[5] - R[2] * R[4]) / det,
+                   (R[5] * R[6] - R[3] * R[8]) / det, (R[0] * R[8] - R[2] * R[6]) / det, (R[2] * R[3] - R[0] * R[5]) / det,
+                   (R[3] * R[7] - R[4] * R[6]) / det, (R[1] * R[6] - R[0] * R[7]) / det, (R[0] * R[4] - R[1] * R[3]) / det};
+  for (int k = 0; k < 9; ++k) o.Rinv[k] = (float)inv[k];
+  for (int k = 0; k < 3; ++k) o.t[k] = t[k];
+  for (int k = 0; k < 4; ++k) o.q[k] = q[k];
+  o.tx = (float)t[0]; o.ty = (float)t[1]; o.tz = (float)t[2];
+}
+
+pm_status pm_add_spatula(pm_sim* sim, int bc, double friction, const float* frames, uint32_t n) {
+  if (!sim || (n > 0 && !frames)) return fail(PM_ERR_INVALID, "NULL argument");
+  if (bc < 0 || bc > 2) return fail(PM_ERR_INVALID, "bc");
+  if ((int)sim->objects.size() >= kMaxObjects) return fail(PM_ERR_CAPACITY, "too many objects");
+  ObjDev o{};
+  o.kind = OBJ_SPATULA; o.bc = bc; o.friction = (float)friction;
+  double t[3] = {0, 0, 0}, q[4] = {1, 0, 0, 0};
+  if (n > 0) {
+    for (int k = 0; k < 3; ++k) t[k] = frames[k];
+    q[0] = frames[6]; q[1] = frames[3]; q[2] = frames[4]; q[3] = frames[5];
+  }
+  pose_from(o, t, q);
+  sim->frames.assign(frames, frames + (size_t)n * 7);
+  sim->objects.push_back(o);
+  sim->knife = (int)sim->objects.size() - 1;
+  sim->prepared = false;
+  return PM_OK;
+}
+
+pm_status pm_add_spatula_file(pm_sim* sim, int bc, double friction, const char* anim_path) {
+  if (!sim || !anim_path) return fail(PM_ERR_INVALID, "NULL argument");
+  std::ifstream f(anim_path, std::ios::binary | std::ios::ate);
+  if (!f) return fail(PM_ERR_IO, std::string("cannot open ") + anim_path);
+  std::streamsize size = f.tellg();
+  f.seekg(0, std::ios::beg);
+  std::vector<float> buf((size_t)size / 28 * 7);
+  if (!f.read(reinterpret_cast<char*>(buf.data()), (std::streamsize)(buf.size() * sizeof(float))))
+    return fail(PM_ERR_IO, std::string("cannot read ") + anim_path);
+  return pm_add_spatula(sim, bc, friction, buf.data(), (uint32_t)(buf.size() / 7));
+}
+
+pm_status pm_add_box_knife(pm_sim* sim, int bc, double friction, const double half[3], const double* waypoints,
+                           uint32_t n, double speed, const double* quat_wxyz) {
+  if (!sim || !half || (n > 0 && !waypoints)) return fail(PM_ERR_INVALID, "NULL argument");
+  if (bc < 0 || bc > 2) return fail(PM_ERR_INVALID, "bc");
+  if (n > (uint32_t)kMaxWaypoints) return fail(PM_ERR_CAPACITY, "too many waypoints");
+  if ((int)sim->objects.size() >= kMaxObjects) return fail(PM_ERR_CAPACITY, "too many objects");
+  ObjDev o{};
+  o.kind = OBJ_BOXKNIFE; o.bc = bc; o.friction = (float)friction;
+  for (int k = 0; k < 3; ++k) o.half[k] = (float)half[k];
+  o.n_waypoints = (int)n;
+  for (uint32_t i = 0; i < n * 3; ++i) o.waypoints[i] = (float)waypoints[i];
+  o.speed = speed;
+  o.s = 0;
+  double t[3] = {0, 0, 0}, q[4] = {1, 0, 0, 0};
+  if (n > 0) for (int k = 0; k < 3; ++k) t[k] = waypoints[k];
+  if (quat_wxyz) for (int k = 0; k < 4; ++k) q[k] = quat_wxyz[k];
+  pose_from(o, t, q);
+  sim->objects.push_back(o);
+  sim->knife = (int)sim->objects.size() - 1;
+  sim->prepared = false;
+  return PM_OK;
+}
+
+pm_status pm_add_ground(pm_sim* sim, int bc, double friction, double y0) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (bc < 0 || bc > 2) return fail(PM_ERR_INVALID, "bc");
+  if ((int)sim->objects.size() >= kMaxObjects) return fail(PM_ERR_CAPACITY, "too many objects");
+  ObjDev o{};
+  o.kind = OBJ_GROUND; o.bc = bc; o.friction = (float)friction; o.y0 = (float)y0;
+  double t[3] = {0, 0, 0}, q[4] = {1, 0, 0, 0};
+  pose_from(o, t, q);
+  sim->objects.push_back(o);
+  sim->prepared = false;
+  return PM_OK;
+}
+
+pm_status pm_add_curve(pm_sim* sim, int bc, double friction) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (bc < 0 || bc > 2) return fail(PM_ERR_INVALID, "bc");
+  if ((int)sim->objects.size() >= kMaxObjects) return fail(PM_ERR_CAPACITY, "too many objects");
+  ObjDev o{};
+  o.kind = OBJ_CURVE; o.bc = bc; o.friction = (float)friction;
+  double t[3] = {0, 0, 0}, q[4] = {1, 0, 0, 0};
+  pose_from(o, t, q);
+  sim->objects.push_back(o);
+  sim->prepared = false;
+  return PM_OK;
+}
+
+pm_status pm_setup_scene(pm_sim* sim, float fps, const char* pigment_config_path, const char* sim_config_path,
+                         const char* anim_path) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (sim->np == 0) return fail(PM_ERR_STATE, "pm_setup_scene needs particles: call pm_set_particles first");
+  pm_status s;
+  if (pigment_config_path && (s = pm_load_pigment_config(sim, pigment_config_path)) != PM_OK) return s;
+  if (sim_config_path && (s = pm_load_sim_config(sim, sim_config_path)) != PM_OK) return s;
+  HostParams& h = sim->hp;  // simulation_units.cpp:82-130
+  h.end_frame = 1800;
+  h.fps = fps;
+  h.gravity[0] = 0.0; h.gravity[1] = -9.81; h.gravity[2] = 0.0;
+  h.use_particle_boundaries = 1;
+  for (int d = 0; d < 3; ++d) { h.pbmin[d] = -2.0; h.pbmax[d] = 2.0; h.grid_ref[d] = 0.0; }
+  if ((s = pm_add_plate(sim, 0.0, PM_PLATE_BOTTOM, PM_BC_SLIPSTICK, 1.0, -1e15, 1e15, 0, 0, 0, 1.0, 0.0)) != PM_OK) return s;
+  if (anim_path && (s = pm_add_spatula_file(sim, PM_BC_SLIPFREE, 0.0, anim_path)) != PM_OK) return s;
+  h.plastic_model = PM_DPVISC;
+  h.use_pradhana = 1;
+  h.q_prefac = 1.0 / std::sqrt(2.0);
+  return PM_OK;
+}
+
+pm_status pm_prepare(pm_sim* sim) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (sim->np == 0) return fail(PM_ERR_STATE, "no particles");
+  HostParams& h = sim->hp;
+  if (!(h.dx > 0) || !(h.particle_mass > 0) || !(h.particle_volume > 0))
+    return fail(PM_ERR_INVALID, "dx, particle_mass and particle_volume must be positive");
+  if (h.plastic_model != PM_NO_PLASTICITY && h.plastic_model != PM_VMVISC && h.plastic_model != PM_DPVISC)
+    return fail(PM_ERR_UNSUPPORTED, "plastic model");
+  CK(cudaSetDevice(sim->device));
+  h.use_musl = 1;  // simulation_units.cpp:185-186
+  // objects and keyframes
+  if (sim->d_frames) { cudaFree(sim->d_frames); sim->d_frames = nullptr; }
+  if (!sim->frames.empty()) {
+    CK(cudaMalloc(&sim->d_frames, sim->frames.size() * sizeof(float)));
+    CK(cudaMemcpy(sim->d_frames, sim->frames.data(), sim->frames.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  Ctrl* c = sim->h_ctrl;
+  const bool first = sim->host_step == 0;
+  if (first) {
+    std::memset(c, 0, sizeof(Ctrl));
+    c->n_plates = (int)sim->plates.size();
+    for (int i = 0; i < c->n_plates; ++i) c->plates[i] = sim->plates[i];
+    c->n_objects = (int)sim->objects.size();
+    for (int i = 0; i < c->n_objects; ++i) c->objects[i] = sim->objects[i];
+    c->knife = sim->knife;
+  } else {
+    pm_status s = sim->sync_ctrl();
+    if (s != PM_OK) return s;
+  }
+  // initial reductions over the particles
+  c->max_v2 = 0;
+  for (int d = 0; d < 3; ++d) { c->xmin_key[d] = 0x7fffffff; c->xmax_key[d] = (int)0x80000000; }
+  c->n_active = 0;
+  pm_status s = sim->push_ctrl();
+  if (s != PM_OK) return s;
+  Params tmp{};
+  tmp.np = (int)sim->np;
+  tmp.np_stride = sim->np_stride;
+  launch_reduce_state(tmp, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], sim->d_ctrl, sim->stream);
+  CK(cudaGetLastError());
+  if ((s = sim->sync_ctrl()) != PM_OK) return s;
+  // remeshFixedInit(2,2,2) (remesh.cpp:45-180), only before the first step
+  if (first) {
+    double mn[3], mx[3];
+    for (int d = 0; d < 3; ++d) {
+      if (c->n_active == 0) { mn[d] = mx[d] = 0.0; }
+      else { mn[d] = fkey_inv(c->xmin_key[d]); mx[d] = fkey_inv(c->xmax_key[d]); }
+    }
+    if (h.grid_ref[0] < 1e10) {
+      for (int d = 0; d < 3; ++d) {
+        if (h.grid_ref[d] < mn[d]) mn[d] = h.grid_ref[d];
+        else if (h.grid_ref[d] > mx[d]) mx[d] = h.grid_ref[d];
+      }
+    }
+    for (int d = 0; d < 3; ++d) {
+      c->min_init[d] = mn[d]; c->max_init[d] = mx[d];
+      c->low_init[d] = mn[d] - 2.0 * h.dx; c->high_init[d] = mx[d] + 2.0 * h.dx;
+      c->low[d] = c->low_init[d]; c->high[d] = c->high_init[d];
+    }
+    c->time = 0; c->frame = 0; c->step = 0;
+  } else {
+    c->time = 0; c->frame = 0;  // prepareSimulation resets time and frame
+  }
+  c->end_frame = (uint32_t)h.end_frame;
+  c->auto_frame = (uint32_t)h.auto_frame;
+  // grid capacity from the initial box with headroom
+  {
+    long long nb = 1;
+    for (int d = 0; d < 3; ++d) {
+      double mn = c->n_active ? fkey_inv(c->xmin_key[d]) : c->low_init[d];
+      double mx = c->n_active ? fkey_inv(c->xmax_key[d]) : c->low_init[d];
+      long long n = (long long)std::ceil((mx - mn) / h.dx) + 8;
+      n = (n + 3) / 4 + 1;
+      nb *= n;
+    }
+    long long want = nb * 2 + 64;
+    if (want * kBrickNodes > 0x7ffffff0LL) want = 0x7ffffff0LL / kBrickNodes;
+    if (sim->brick_cap < want) {
+      if ((s = sim->alloc_grid((int)want)) != PM_OK) return s;
+    }
+  }
+  sim->prepared = true;
+  sim->fill_params();
+  if ((s = sim->push_ctrl()) != PM_OK) return s;
+  return PM_OK;
+}
+
+pm_status pm_step(pm_sim* sim) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (!sim->prepared) return fail(PM_ERR_STATE, "call pm_prepare first");
+  CK(cudaSetDevice(sim->device));
+  // one reference step(): no frame bookkeeping even when auto_frame is set
+  pm_status s;
+  const uint32_t af = sim->h_ctrl->auto_frame;
+  if (af) {
+    if ((s = sim->sync_ctrl()) != PM_OK) return s;
+    sim->h_ctrl->auto_frame = 0;
+    if ((s = sim->push_ctrl()) != PM_OK) return s;
+  }
+  s = sim->run_steps(1, false);
+  if (af) {
+    sim->h_ctrl->auto_frame = af;
+    pm_status s2 = sim->push_ctrl();
+    if (s == PM_OK) s = s2;
+  }
+  return s;
+}
+
+pm_status pm_advance(pm_sim* sim, uint32_t nsteps, uint32_t* frames_done) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (!sim->prepared) return fail(PM_ERR_STATE, "call pm_prepare first");
+  CK(cudaSetDevice(sim->device));
+  pm_status s = sim->sync_ctrl();
+  if (s != PM_OK) return s;
+  const uint32_t fd0 = sim->h_ctrl->frames_done;
+  const uint32_t af = sim->h_ctrl->auto_frame;
+  if (!af) { sim->h_ctrl->auto_frame = 1; if ((s = sim->push_ctrl()) != PM_OK) return s; }
+  s = sim->run_steps(nsteps, true);
+  if (!af) { sim->h_ctrl->auto_frame = 0; pm_status s2 = sim->push_ctrl(); if (s == PM_OK) s = s2; }
+  if (frames_done) *frames_done = sim->h_ctrl->frames_done - fd0;
+  return s;
+}
+
+pm_status pm_frame_finished(pm_sim* sim, int* finished) {
+  if (!sim || !finished) return fail(PM_ERR_INVALID, "NULL argument");
+  pm_status s = sim->sync_ctrl();
+  if (s != PM_OK) return s;
+  Ctrl* c = sim->h_ctrl;
+  const double frame_dt = 1.0 / sim->hp.fps;
+  *finished = 0;
+  if (frame_dt * (double)(c->frame + 1) - c->time < sim->hp.min_dt * 1.1) {
+    c->frame += 1;
+    *finished = 1;
+    return sim->push_ctrl();
+  }
+  return PM_OK;
+}
+
+pm_status pm_is_finished(pm_sim* sim, int* finished) {
+  if (!sim || !finished) return fail(PM_ERR_INVALID, "NULL argument");
+  pm_status s = sim->sync_ctrl();
+  if (s != PM_OK) return s;
+  const double final_time = sim->hp.end_frame / sim->hp.fps;
+  *finished = (sim->h_ctrl->frame >= (uint32_t)sim->hp.end_frame || sim->h_ctrl->time >= final_time) ? 1 : 0;
+  return PM_OK;
+}
+
+pm_status pm_get_grid_boundaries(pm_sim* sim, double lo[3], double hi[3]) {
+  if (!sim || !lo || !hi) return fail(PM_ERR_INVALID, "NULL argument");
+  if (sim->prepared) { pm_status s = sim->sync_ctrl(); if (s != PM_OK) return s; }
+  for (int d = 0; d < 3; ++d) { lo[d] = sim->h_ctrl->low[d]; hi[d] = sim->h_ctrl->high[d]; }
+  return PM_OK;
+}
+
+pm_status pm_get_knife(pm_sim* sim, int* exists, double inv[16], double half_dims[3]) {
+  if (!sim || !exists) return fail(PM_ERR_INVALID, "NULL argument");
+  *exists = 0;
+  if (sim->knife < 0) return PM_OK;
+  const ObjDev* o = &sim->objects[sim->knife];
+  if (sim->prepared) {
+    pm_status s = sim->sync_ctrl();
+    if (s != PM_OK) return s;
+    o = &sim->h_ctrl->objects[sim->knife];
+  }
+  *exists = 1;
+  if (inv) {
+    double R[9];
+    for (int k = 0; k < 9; ++k) R[k] = o->Rinv[k];
+    for (int r = 0; r < 3; ++r) {
+      for (int q = 0; q < 3; ++q) inv[4 * r + q] = R[3 * r + q];
+      inv[4 * r + 3] = -(R[3 * r] * o->t[0] + R[3 * r + 1] * o->t[1] + R[3 * r + 2] * o->t[2]);
+    }
+    inv[12] = inv[13] = inv[14] = 0; inv[15] = 1;
+  }
+  if (half_dims) {  // MPMIntegrationSim.cpp:161-168: (halfWidth, halfThickness, halfLength)
+    if (o->kind == OBJ_SPATULA) { half_dims[0] = 0.368; half_dims[1] = 0.07; half_dims[2] = 0.736; }
+    else for (int k = 0; k < 3; ++k) half_dims[k] = o->half[k];
+  }
+  return PM_OK;
+}
+
+pm_status pm_get_error_flags(pm_sim* sim, uint32_t* flags, int clear) {
+  if (!sim || !flags) return fail(PM_ERR_INVALID, "NULL argument");
+  pm_status s = sim->sync_ctrl();
+  if (s != PM_OK) return s;
+  *flags = sim->h_ctrl->error_flags;
+  if (clear) { sim->h_ctrl->error_flags = 0; return sim->push_ctrl(); }
+  return PM_OK;
+}
+
+pm_status pm_get_stats(pm_sim* sim, double* total_mass, double momentum[3], double mean_latent[7], uint32_t* n_active) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (sim->np == 0) return PM_OK;
+  CK(cudaSetDevice(sim->device));
+  CK(cudaMemsetAsync(sim->d_stats, 0, 16 * sizeof(double), sim->stream));
+  Params p = sim->P;
+  p.np = (int)sim->np;
+  p.np_stride = sim->np_stride;
+  launch_stats(p, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], sim->d_stats, sim->stream);
+  CK(cudaGetLastError());
+  double h[16];
+  CK(cudaMemcpyAsync(h, sim->d_stats, sizeof(h), cudaMemcpyDeviceToHost, sim->stream));
+  CK(cudaStreamSynchronize(sim->stream));
+  const double mp = sim->hp.particle_mass;
+  if (total_mass) *total_mass = h[0] * mp;
+  if (momentum) for (int d = 0; d < 3; ++d) momentum[d] = h[1 + d] * mp;
+  if (mean_latent) for (int k = 0; k < 7; ++k) mean_latent[k] = h[0] > 0 ? h[4 + k] / h[0] : 0.0;
+  if (n_active) *n_active = (uint32_t)h[0];
+  return PM_OK;
+}
+
+pm_status pm_get_grid(pm_sim* sim, double origin[3], uint32_t dims[3], float* mass, float* v_update, float* v_musl,
+                      float* flip, float* latent, float* shear) {
+  if (!sim || !origin || !dims) return fail(PM_ERR_INVALID, "NULL argument");
+  if (!sim->prepared) return fail(PM_ERR_STATE, "not prepared");
+  pm_status s = sim->sync_ctrl();
+  if (s != PM_OK) return s;
+  const Ctrl* c = sim->h_ctrl;
+  for (int d = 0; d < 3; ++d) {
+    origin[d] = sim->P.anchor_d[d] + (double)c->g0[d] * sim->hp.dx;
+    dims[d] = (uint32_t)c->dims[d];
+  }
+  if (!mass && !v_update && !v_musl && !flip && !latent && !shear) return PM_OK;
+  const size_t nn = (size_t)c->n_nodes;
+  std::vector<float4> g(nn * 4), m(nn);
+  CK(cudaMemcpyAsync(g.data(), sim->d_grid, nn * 4 * sizeof(float4), cudaMemcpyDeviceToHost, sim->stream));
+  CK(cudaMemcpyAsync(m.data(), sim->d_gmusl, nn * sizeof(float4), cudaMemcpyDeviceToHost, sim->stream));
+  CK(cudaStreamSynchronize(sim->stream));
+  for (int i = 0; i < c->dims[0]; ++i)
+    for (int j = 0; j < c->dims[1]; ++j)
+      for (int k = 0; k < c->dims[2]; ++k) {
+        const size_t l = ((size_t)i * c->dims[1] + j) * c->dims[2] + k;
+        const size_t b = ((size_t)(i >> 2) * c->nb[1] + (j >> 2)) * c->nb[2] + (k >> 2);
+        const size_t n = b * kBrickNodes + (i & 3) * 16 + (j & 3) * 4 + (k & 3);
+        const float4 r0 = g[n * 4], r1 = g[n * 4 + 1], r2 = g[n * 4 + 2], r3 = g[n * 4 + 3];
+        const bool has = r0.x > 0.f;
+        if (mass) mass[l] = has ? r0.x : 0.f;
+        if (v_update) { v_update[3 * l] = has ? r0.y : 0.f; v_update[3 * l + 1] = has ? r0.z : 0.f; v_update[3 * l + 2] = has ? r0.w : 0.f; }
+        if (flip) { flip[3 * l] = has ? r1.x : 0.f; flip[3 * l + 1] = has ? r1.y : 0.f; flip[3 * l + 2] = has ? r1.z : 0.f; }
+        if (latent) {
+          const float lv[7] = {r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y};
+          for (int q = 0; q < 7; ++q) latent[7 * l + q] = has ? lv[q] : 0.f;
+        }
+        if (shear) shear[l] = has ? r3.z : 0.f;
+        if (v_musl) {
+          const float4 mm = m[n];
+          const float inv = mm.w > 0.f ? 1.f / mm.w : 0.f;
+          v_musl[3 * l] = mm.x * inv; v_musl[3 * l + 1] = mm.y * inv; v_musl[3 * l + 2] = mm.z * inv;
+        }
+      }
+  return PM_OK;
+}
+
+pm_status pm_set_return_map(pm_sim* sim, int mode) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (mode != PM_RETURN_MAP_PLAIN && mode != PM_RETURN_MAP_SURROGATE) return fail(PM_ERR_INVALID, "mode");
+  if (mode == PM_RETURN_MAP_SURROGATE && !sim->d_mlp)
+    return fail(PM_ERR_STATE, "no surrogate weights loaded");
+  sim->return_map = mode;
+  if (sim->prepared) sim->fill_params();
+  return PM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1503 @@
+// sm_100a kernels of the paint-mixing MPM step.
+//
+// One step (the reference's Simulation::advanceStep, matter/src/simulation/simulation.cpp:225-280):
+//   k_prologue      dt (update_dt.cpp:5-41) and the step's grid box (remesh.cpp:182-297)
+//   k_clear         zero cell counters and the main grid records
+//   k_count         per particle: cell key + rank (counting sort, pass 1)
+//   k_scan_*        exclusive prefix of the cell counters -> cell starts
+//   k_scatter       counting sort, pass 2: new position -> read index
+//   k_p2g           P2G + particle half of the explicit update (p2g.cpp:6-126,
+//                   explicit_euler_update.cpp:12-55) with the cached Kirchhoff stress
+//   k_grid_update   grid half of the explicit update + collisions
+//                   (explicit_euler_update.cpp:61-110, boundary_collision.cpp:5-316)
+//   k_g2p_musl      G2P + pigment mixing + MUSL velocity update and re-scatter
+//                   (g2p.cpp:12-135, musl.cpp:6-98)
+//   k_defgrad       deformation update + FP64 SVD/return map + position update + stress cache
+//                   + reductions for the next step (deformation_update.cpp, plasticity.cpp:18-340,
+//                   position_update.cpp:6-91, simulation.hpp:287-294)
+//   k_epilogue      moveObjects (simulation.cpp:284-291), time += dt, frame bookkeeping
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cmath>
+#include "pm_internal.cuh"
+#include "pm_launch.h"
+
+namespace pm {
+
+// ------------------------------------------------------------------------------------------
+// helpers
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ int cell_of(float x, float anchor, float inv_dx) {
+  // base node of the 3-node quadratic stencil; the exact same float ops everywhere
+  return (int)floorf(__fsub_rn(__fmul_rn(__fsub_rn(x, anchor), inv_dx), 0.5f));
+}
+__device__ __forceinline__ float node_pos(int g, float anchor, float dx) {
+  return __fadd_rn(anchor, __fmul_rn((float)g, dx));
+}
+// quadratic B-spline and derivative, tools.hpp:153-177
+__device__ __forceinline__ float bsN(float u) {
+  float a = fabsf(u);
+  if (a < 0.5f) return 0.75f - a * a;
+  if (a < 1.5f) return 0.5f * (1.5f - a) * (1.5f - a);
+  return 0.f;
+}
+__device__ __forceinline__ float bsdN(float u) {
+  float a = fabsf(u);
+  if (a < 0.5f) return -2.f * u;
+  if (a < 1.5f) return u - 1.5f * (float)((0.f < u) - (u < 0.f));
+  return 0.f;
+}
+
+__device__ __forceinline__ void red_add_v4(float4* addr, float a, float b, float c, float d) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
+               : "memory");
+}
+
+struct AxisW {
+  int base;       // lattice index of the stencil's first node
+  float N[3];     // weights at base+0..2
+  float dN[3];    // derivative * inv_dx
+  float r;        // x - node_pos(base)
+};
+
+__device__ __forceinline__ AxisW axis_weights(float x, float anchor, float dx, float inv_dx) {
+  AxisW a;
+  a.base = cell_of(x, anchor, inv_dx);
+  float x0 = node_pos(a.base, anchor, dx);
+  a.r = x - x0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float xi = node_pos(a.base + k, anchor, dx);
+    float u = (x - xi) * inv_dx;
+    a.N[k] = bsN(u);
+    a.dN[k] = bsdN(u) * inv_dx;
+  }
+  return a;
+}
+
+__device__ __forceinline__ const Ctrl* C_(const Bufs& B) { return B.ctrl; }
+
+// ------------------------------------------------------------------------------------------
+// 1-thread control kernels
+// ------------------------------------------------------------------------------------------
+__device__ void grid_box_from_aabb(const Params& P, Ctrl* c) {
+  // node range covering every particle's stencil, with a 1-node margin
+  int lo[3], hi[3];
+  for (int d = 0; d < 3; ++d) {
+    float mn = fkey_inv(c->xmin_key[d]), mx = fkey_inv(c->xmax_key[d]);
+    if (c->n_active == 0) { mn = mx = P.anchor[d]; }
+    lo[d] = cell_of(mn, P.anchor[d], P.inv_dx) - 1;
+    hi[d] = cell_of(mx, P.anchor[d], P.inv_dx) + 3;
+  }
+  long long nbricks = 1;
+  for (int d = 0; d < 3; ++d) {
+    int n = hi[d] - lo[d] + 1;
+    n = (n + kBrick - 1) / kBrick * kBrick;
+    c->g0[d] = lo[d];
+    c->dims[d] = n;
+    c->nb[d] = n / kBrick;
+    nbricks *= c->nb[d];
+  }
+  if (nbricks > P.brick_cap) {
+    c->halt = 1;
+    c->need_bricks = (uint32_t)(nbricks > 0x7fffffffLL ? 0x7fffffff : nbricks);
+    c->error_flags |= E_CAPACITY;
+    c->n_bricks = 0;
+    c->n_nodes = 0;
+    return;
+  }
+  c->n_bricks = (int)nbricks;
+  c->n_nodes = (int)nbricks * kBrickNodes;
+}
+
+__global__ void k_prologue(Params P, Bufs B) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  // updateDt (update_dt.cpp:5-41)
+  float m2f = __uint_as_float(c->max_v2);
+  double ms = sqrt((double)m2f);
+  double dt;
+  if (fabs(ms) > 1e-10) dt = fmin(P.cfl * P.dx_d / ms, P.dt_max);
+  else dt = P.dt_max;
+  dt = fmin(dt, P.frame_dt * (double)(c->frame + 1) - c->time);
+  dt = fmax(dt, P.min_dt);
+  c->dt = dt;
+  // reference grid boundaries (remeshFixedCont, remesh.cpp:182-297); step 0 keeps the init box
+  if (c->step > 0) {
+    for (int d = 0; d < 3; ++d) {
+      double mn = fkey_inv(c->xmin_key[d]), mx = fkey_inv(c->xmax_key[d]);
+      if (c->n_active == 0) mn = mx = 0.0;
+      double dxd = P.dx_d;
+      if (mx < c->max_init[d]) {
+        double r = floor(fmax(0.0, (c->max_init[d] - mx) / dxd - 1e-8 * dxd));
+        c->high[d] = c->high_init[d] - r * dxd;
+      } else {
+        double e = floor(fmax(0.0, (mx - c->max_init[d]) / dxd - 1e-8 * dxd));
+        c->high[d] = c->high_init[d] + e * dxd;
+      }
+      if (mn > c->min_init[d]) {
+        double r = floor(fmax(0.0, (mn - c->min_init[d]) / dxd - 1e-8 * dxd));
+        c->low[d] = c->low_init[d] + r * dxd;
+      } else {
+        double e = floor(fmax(0.0, (c->min_init[d] - mn) / dxd - 1e-8 * dxd));
+        c->low[d] = c->low_init[d] - e * dxd;
+      }
+    }
+  }
+  grid_box_from_aabb(P, c);
+  if (c->halt) return;  // keep the reductions: the host regrows the grid and re-runs this step
+  // reset the reductions that this step's k_defgrad fills
+  c->max_v2 = 0u;
+  for (int d = 0; d < 3; ++d) { c->xmin_key[d] = 0x7fffffff; c->xmax_key[d] = (int)0x80000000; }
+  c->n_active = 0;
+  c->plastic_count = 0;
+}
+
+// quaternion helpers (w, x, y, z)
+__device__ void q_to_rot(const double q[4], double R[9]) {
+  double n = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  double w = q[0] / n, x = q[1] / n, y = q[2] / n, z = q[3] / n;
+  R[0] = 1 - 2 * (y * y + z * z); R[1] = 2 * (x * y - z * w); R[2] = 2 * (x * z + y * w);
+  R[3] = 2 * (x * y + z * w); R[4] = 1 - 2 * (x * x + z * z); R[5] = 2 * (y * z - x * w);
+  R[6] = 2 * (x * z - y * w); R[7] = 2 * (y * z + x * w); R[8] = 1 - 2 * (x * x + y * y);
+}
+__device__ void set_pose(ObjDev& o, const double t[3], const double q[4]) {
+  for (int k = 0; k < 3; ++k) o.t[k] = t[k];
+  for (int k = 0; k < 4; ++k) o.q[k] = q[k];
+  double R[9];
+  q_to_rot(q, R);
+  double det = R[0] * (R[4] * R[8] - R[5] * R[7]) - R[1] * (R[3] * R[8] - R[5] * R[6]) + R[2] * (R[3] * R[7] - R[4] * R[6]);
+  double inv[9];
+  inv[0] = (R[4] * R[8] - R[5] * R[7]) / det;
+  inv[1] = (R[2] * R[7] - R[1] * R[8]) / det;
+  inv[2] = (R[1] * R[5] - R[2] * R[4]) / det;
+  inv[3] = (R[5] * R[6] - R[3] * R[8]) / det;
+  inv[4] = (R[0] * R[8] - R[2] * R[6]) / det;
+  inv[5] = (R[2] * R[3] - R[0] * R[5]) / det;
+  inv[6] = (R[3] * R[7] - R[4] * R[6]) / det;
+  inv[7] = (R[1] * R[6] - R[0] * R[7]) / det;
+  inv[8] = (R[0] * R[4] - R[1] * R[3]) / det;
+  for (int k = 0; k < 9; ++k) o.Rinv[k] = (float)inv[k];
+  o.tx = (float)t[0]; o.ty = (float)t[1]; o.tz = (float)t[2];
+}
+__device__ void slerp_d(const double a[4], const double b[4], double t, double out[4]) {
+  const double one = 1.0 - 2.220446049250313e-16;
+  double d = a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
+  double ad = fabs(d), s0, s1;
+  if (ad >= one) { s0 = 1.0 - t; s1 = t; }
+  else {
+    double th = acos(ad), sth = sin(th);
+    s0 = sin((1.0 - t) * th) / sth;
+    s1 = sin(t * th) / sth;
+  }
+  if (d < 0) s1 = -s1;
+  for (int k = 0; k < 4; ++k) out[k] = s0 * a[k] + s1 * b[k];
+}
+
+__device__ void move_knife(const Params& P, ObjDev& o, double dt) {
+  if (o.kind == OBJ_SPATULA) {  // object_spatula.hpp:164-233
+    o.current_time += dt;
+    if (P.n_frames <= 0) {
+      for (int k = 0; k < 3; ++k) { o.vlin[k] = 0.f; o.omega[k] = 0.f; }
+      return;
+    }
+    double fi = o.current_time * 60.0;
+    int i0u = (int)floor(fi);
+    int i0 = min(i0u, P.n_frames - 1), i1 = min(i0u + 1, P.n_frames - 1);
+    i0 = max(i0, 0); i1 = max(i1, 0);
+    double tt = fi - (double)i0u;
+    const float* f0 = P.frames + 7 * i0;
+    const float* f1 = P.frames + 7 * i1;
+    double pi[3];
+    for (int k = 0; k < 3; ++k) pi[k] = (double)f0[k] + tt * ((double)f1[k] - (double)f0[k]);
+    double q0[4] = {f0[6], f0[3], f0[4], f0[5]}, q1[4] = {f1[6], f1[3], f1[4], f1[5]};
+    double qi[4];
+    slerp_d(q0, q1, tt, qi);
+    for (int k = 0; k < 3; ++k) o.vlin[k] = (float)((pi[k] - o.t[k]) / dt);
+    // relative rotation dq = qi * conj(q_old) -> axis angle (angle in [0, pi])
+    const double* a = qi;
+    double b[4] = {o.q[0], -o.q[1], -o.q[2], -o.q[3]};
+    double dq[4] = {a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3],
+                    a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2],
+                    a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1],
+                    a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0]};
+    double n2 = dq[1] * dq[1] + dq[2] * dq[2] + dq[3] * dq[3];
+    if (n2 == 0.0) { for (int k = 0; k < 3; ++k) o.omega[k] = 0.f; }
+    else {
+      double vn = sqrt(n2);
+      double ang = 2.0 * atan2(vn, fabs(dq[0]));
+      double sg = dq[0] < 0 ? -1.0 : 1.0;
+      for (int k = 0; k < 3; ++k) o.omega[k] = (float)(dq[k + 1] * (sg * ang / (vn * dt)));
+    }
+    set_pose(o, pi, qi);
+  } else if (o.kind == OBJ_BOXKNIFE) {
+    o.s += o.speed * dt;
+    double pn[3] = {o.t[0], o.t[1], o.t[2]};
+    if (o.n_waypoints > 0) {
+      double acc = 0.0;
+      bool found = false;
+      for (int i = 0; i + 1 < o.n_waypoints && !found; ++i) {
+        double d[3], L = 0.0;
+        for (int k = 0; k < 3; ++k) { d[k] = (double)o.waypoints[3 * (i + 1) + k] - (double)o.waypoints[3 * i + k]; L += d[k] * d[k]; }
+        L = sqrt(L);
+        if (o.s <= acc + L && L > 0) {
+          for (int k = 0; k < 3; ++k) pn[k] = (double)o.waypoints[3 * i + k] + d[k] * ((o.s - acc) / L);
+          found = true;
+        }
+        acc += L;
+      }
+      if (!found) for (int k = 0; k < 3; ++k) pn[k] = (double)o.waypoints[3 * (o.n_waypoints - 1) + k];
+    }
+    for (int k = 0; k < 3; ++k) { o.vlin[k] = (float)((pn[k] - o.t[k]) / dt); o.omega[k] = 0.f; }
+    double q[4] = {o.q[0], o.q[1], o.q[2], o.q[3]};
+    set_pose(o, pn, q);
+  }
+}
+
+__global__ void k_epilogue(Params P, Bufs B) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  double dt = c->dt;
+  // moveObjects (simulation.cpp:284-291): plates, then the spatula
+  for (int i = 0; i < c->n_plates; ++i) {  // object_plate.hpp:136-162
+    PlateDev& pl = c->plates[i];
+    double factor = (c->time < (double)pl.load_factor * P.frame_dt) ? (1.0 / (double)pl.vmin_factor) : 1.0;
+    pl.vx = (float)(pl.vx0 * factor); pl.vy = (float)(pl.vy0 * factor); pl.vz = (float)(pl.vz0 * factor);
+    if (pl.type == PT_LEFT || pl.type == PT_RIGHT) { pl.pos += dt * pl.vx; pl.upper += dt * pl.vy; pl.lower += dt * pl.vy; }
+    else if (pl.type == PT_BOTTOM || pl.type == PT_TOP) { pl.pos += dt * pl.vy; pl.upper += dt * pl.vx; pl.lower += dt * pl.vx; }
+    else pl.pos += dt * pl.vz;
+  }
+  if (c->knife >= 0) move_knife(P, c->objects[c->knife], dt);
+  c->time += dt;
+  c->step += 1;
+  if (c->auto_frame) {  // frameFinished (simulation_units.cpp:235-241)
+    if (P.frame_dt * (double)(c->frame + 1) - c->time < P.min_dt * 1.1) { c->frame += 1; c->frames_done += 1; }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// counting sort by cell
+// ------------------------------------------------------------------------------------------
+__global__ void k_clear(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  const int nn = c->n_nodes;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn + 2; i += stride) B.cell[i] = 0u;
+  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn * 4; i += stride) B.grid[i] = z;
+}
+
+__device__ __forceinline__ uint32_t brick_key(const int c[3], const Ctrl* ctrl) {
+  int bx = c[0] >> 2, by = c[1] >> 2, bz = c[2] >> 2;
+  int lx = c[0] & 3, ly = c[1] & 3, lz = c[2] & 3;
+  return (uint32_t)(((bx * ctrl->nb[1] + by) * ctrl->nb[2] + bz) * kBrickNodes + lx * 16 + ly * 4 + lz);
+}
+
+__global__ void k_count(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  const int np = P.np, S = P.np_stride;
+  const uint32_t inactive_key = (uint32_t)c->n_nodes;
+  const int stride = gridDim.x * blockDim.x;
+  bool range_err = false;
+  for (int base = blockIdx.x * blockDim.x; base < np; base += stride) {
+    int p = base + threadIdx.x;
+    bool valid = p < np;
+    uint32_t key = 0xffffffffu;
+    if (valid) {
+      uint32_t meta = B.meta_in[p];
+      if (meta & kInactiveBit) key = inactive_key;
+      else {
+        int cc[3];
+        for (int d = 0; d < 3; ++d) {
+          float x = B.pin[(F_X + d) * S + p];
+          int g = cell_of(x, P.anchor[d], P.inv_dx) - c->g0[d];
+          if (g < 0 || g + 2 >= c->dims[d]) { range_err = true; g = min(max(g, 0), c->dims[d] - 3); }
+          cc[d] = g;
+        }
+        key = brick_key(cc, c);
+      }
+    }
+    // warp-aggregated rank: lanes sharing a key take consecutive ranks from one atomic
+    unsigned am = __ballot_sync(0xffffffffu, valid);
+    if (valid) {
+      unsigned peers = __match_any_sync(am, key);
+      int leader = __ffs(peers) - 1;
+      int lane = threadIdx.x & 31;
+      uint32_t r0 = 0;
+      if (lane == leader) r0 = atomicAdd(&B.cell[key], (uint32_t)__popc(peers));
+      r0 = __shfl_sync(peers, r0, leader);
+      B.key[p] = key;
+      B.rank[p] = r0 + __popc(peers & ((1u << lane) - 1u));
+    }
+  }
+  if (range_err) atomicOr(&B.ctrl->error_flags, (uint32_t)E_INDEX_RANGE);
+}
+
+// Exclusive scan of cell[0 .. n_nodes+1) in 4096-entry blocks.
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 4;
+constexpr int kScanBlock = kScanThreads * kScanPer;
+
+__device__ __forceinline__ uint32_t block_incl_scan(uint32_t v, uint32_t* warp_sums) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  if (lane == 31) warp_sums[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t s = warp_sums[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t t = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += t;
+    }
+    warp_sums[lane] = s;
+  }
+  __syncthreads();
+  if (wid > 0) v += warp_sums[wid - 1];
+  return v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_local(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  const int n = c->n_nodes + 1;
+  const int b0 = blockIdx.x * kScanBlock;
+  if (b0 >= n) return;
+  __shared__ uint32_t ws[32];
+  uint32_t v[kScanPer];
+  uint32_t tsum = 0;
+  const int i0 = b0 + threadIdx.x * kScanPer;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) { v[k] = (i0 + k < n) ? B.cell[i0 + k] : 0u; tsum += v[k]; }
+  uint32_t incl = block_incl_scan(tsum, ws);
+  uint32_t run = incl - tsum;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    if (i0 + k < n) B.cell[i0 + k] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == kScanThreads - 1) B.scan_part[blockIdx.x] = incl;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_top(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  const int n = c->n_nodes + 1;
+  const int nblk = (n + kScanBlock - 1) / kScanBlock;
+  __shared__ uint32_t ws[32];
+  __shared__ uint32_t carry_s;
+  if (threadIdx.x == 0) carry_s = 0;
+  __syncthreads();
+  for (int s0 = 0; s0 < nblk; s0 += kScanThreads) {
+    int i = s0 + threadIdx.x;
+    uint32_t v = i < nblk ? B.scan_part[i] : 0u;
+    uint32_t incl = block_incl_scan(v, ws);
+    uint32_t carry = carry_s;
+    if (i < nblk) B.scan_part[i] = carry + incl - v;
+    __syncthreads();
+    if (threadIdx.x == kScanThreads - 1) carry_s = carry + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) B.cell[n] = carry_s;  // total = np
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_add(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  const int n = c->n_nodes + 1;
+  const int b0 = blockIdx.x * kScanBlock;
+  if (b0 >= n || blockIdx.x == 0) return;
+  const uint32_t off = B.scan_part[blockIdx.x];
+  for (int i = b0 + threadIdx.x; i < min(b0 + kScanBlock, n); i += kScanThreads) B.cell[i] += off;
+}
+
+__global__ void k_scatter(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  const int stride = gridDim.x * blockDim.x;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.np; p += stride)
+    B.sorted[B.cell[B.key[p]] + B.rank[p]] = (uint32_t)p;
+}
+
+// ------------------------------------------------------------------------------------------
+// P2G: warp per cell, lane per stencil node, shared 6x6x6 tile per brick
+// ------------------------------------------------------------------------------------------
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kP2GCh = 15;
+
+struct __align__(16) StageP2G {
+  float N[9];     // Nx[3], Ny[3], Nz[3]
+  float dN[9];    // dNx, dNy, dNz (times inv_dx)
+  float q[3];     // v - D * B r
+  float Cc[9];    // D * dx * B columns: C0 xyz, C1 xyz, C2 xyz
+  float tau[6];   // xx yy zz xy xz yz
+  float lat[7];
+  float diff;
+  float pad[4];
+};
+static_assert(sizeof(StageP2G) == 48 * 4, "stage size");
+
+size_t p2g_smem_bytes() { return sizeof(float) * kP2GCh * kTileNodes + sizeof(StageP2G) * kThreads; }
+
+__device__ __forceinline__ void brick_coords(int b, const Ctrl* c, int& bx, int& by, int& bz) {
+  const int nyz = c->nb[1] * c->nb[2];
+  bx = b / nyz;
+  int r = b - bx * nyz;
+  by = r / c->nb[2];
+  bz = r - by * c->nb[2];
+}
+
+__device__ __forceinline__ int tile_to_node(int tn, int bx, int by, int bz, const Ctrl* c) {
+  int tx = tn / 36, ty = (tn / 6) % 6, tz = tn % 6;
+  int gx = bx + (tx >> 2), gy = by + (ty >> 2), gz = bz + (tz >> 2);
+  if (gx >= c->nb[0] || gy >= c->nb[1] || gz >= c->nb[2]) return -1;
+  return ((gx * c->nb[1] + gy) * c->nb[2] + gz) * kBrickNodes + (tx & 3) * 16 + (ty & 3) * 4 + (tz & 3);
+}
+
+__global__ void __launch_bounds__(kThreads) k_p2g(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* tile = reinterpret_cast<float*>(smem_raw);                       // [kP2GCh][216]
+  StageP2G* st = reinterpret_cast<StageP2G*>(tile + kP2GCh * kTileNodes);  // [kThreads]
+  const int S = P.np_stride;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int la = lane / 9, lb = (lane / 3) % 3, lc = lane % 3;
+  const float D = P.apicD, dx = P.dx;
+  const bool apic = P.flip_ratio < 0.f;
+  const int nbr = c->n_bricks;
+  for (int b = blockIdx.x; b < nbr; b += gridDim.x) {
+    const uint32_t* cs = B.cell + (size_t)b * kBrickNodes;
+    const uint32_t ps = cs[0], pe = cs[kBrickNodes];
+    if (ps == pe) continue;
+    int bx, by, bz;
+    brick_coords(b, c, bx, by, bz);
+    for (int i = threadIdx.x; i < kP2GCh * kTileNodes; i += kThreads) tile[i] = 0.f;
+    for (uint32_t c0 = ps; c0 < pe; c0 += kThreads) {
+      const uint32_t c1 = min(c0 + (uint32_t)kThreads, pe);
+      __syncthreads();  // tile zeroed / previous chunk consumed
+      if (c0 + threadIdx.x < c1) {
+        const uint32_t o = B.sorted[c0 + threadIdx.x];
+        StageP2G& s = st[threadIdx.x];
+        float xp[3], r[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          xp[d] = B.pin[(F_X + d) * S + o];
+          AxisW aw = axis_weights(xp[d], P.anchor[d], dx, P.inv_dx);
+          r[d] = aw.r;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) { s.N[3 * d + k] = aw.N[k]; s.dN[3 * d + k] = aw.dN[k]; }
+        }
+        float v[3], Bm[9];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) v[d] = B.pin[(F_V + d) * S + o];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Bm[k] = apic ? B.pin[(F_B + k) * S + o] : 0.f;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          float Br = Bm[3 * i] * r[0] + Bm[3 * i + 1] * r[1] + Bm[3 * i + 2] * r[2];
+          s.q[i] = v[i] - D * Br;
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int i = 0; i < 3; ++i) s.Cc[3 * k + i] = D * dx * Bm[3 * i + k];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s.tau[k] = B.pin[(F_TAU + k) * S + o];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) s.lat[k] = B.pin[(F_LAT + k) * S + o];
+        s.diff = B.pin[F_DIFF * S + o];
+      }
+      __syncthreads();
+      for (int cl = warp; cl < kBrickNodes; cl += kWarps) {
+        const uint32_t s0 = max(cs[cl], c0), s1 = min(cs[cl + 1], c1);
+        if (s0 >= s1) continue;
+        if (lane < 27) {
+          float acc[kP2GCh];
+#pragma unroll
+          for (int k = 0; k < kP2GCh; ++k) acc[k] = 0.f;
+          const float fa = (float)la, fb = (float)lb, fc = (float)lc;
+          for (uint32_t sp = s0; sp < s1; ++sp) {
+            const StageP2G& s = st[sp - c0];
+            const float nx = s.N[la], ny = s.N[3 + lb], nz = s.N[6 + lc];
+            const float nyz = ny * nz;
+            const float w = nx * nyz;
+            const float gx = s.dN[la] * nyz, gy = nx * s.dN[3 + lb] * nz, gz = nx * ny * s.dN[6 + lc];
+            const float wm = w > 1e-25f ? w : 0.f;  // p2g.cpp:39
+            acc[0] += wm;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+              float t = s.q[i] + fa * s.Cc[i] + fb * s.Cc[3 + i] + fc * s.Cc[6 + i];
+              acc[1 + i] += wm * t;
+            }
+            acc[4] += s.tau[0] * gx + s.tau[3] * gy + s.tau[4] * gz;
+            acc[5] += s.tau[3] * gx + s.tau[1] * gy + s.tau[5] * gz;
+            acc[6] += s.tau[4] * gx + s.tau[5] * gy + s.tau[2] * gz;
+#pragma unroll
+            for (int k = 0; k < 7; ++k) acc[7 + k] += wm * s.lat[k];
+            acc[14] += wm * s.diff;
+          }
+          const int lx = cl >> 4, ly = (cl >> 2) & 3, lz = cl & 3;
+          const int tn = ((lx + la) * kTile + (ly + lb)) * kTile + (lz + lc);
+#pragma unroll
+          for (int k = 0; k < kP2GCh; ++k)
+            if (acc[k] != 0.f) atomicAdd(&tile[k * kTileNodes + tn], acc[k]);
+        }
+      }
+    }
+    __syncthreads();
+    for (int tn = threadIdx.x; tn < kTileNodes; tn += kThreads) {
+      const float m = tile[tn];
+      if (m == 0.f) continue;
+      const int node = tile_to_node(tn, bx, by, bz, c);
+      if (node < 0) continue;
+      float4* rec = B.grid + (size_t)node * 4;
+      const float* t = tile + tn;
+      red_add_v4(rec + 0, m, t[1 * kTileNodes], t[2 * kTileNodes], t[3 * kTileNodes]);
+      red_add_v4(rec + 1, t[4 * kTileNodes], t[5 * kTileNodes], t[6 * kTileNodes], t[7 * kTileNodes]);
+      red_add_v4(rec + 2, t[8 * kTileNodes], t[9 * kTileNodes], t[10 * kTileNodes], t[11 * kTileNodes]);
+      red_add_v4(rec + 3, t[12 * kTileNodes], t[13 * kTileNodes], t[14 * kTileNodes], 0.f);
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// grid update with collisions
+// ------------------------------------------------------------------------------------------
+__device__ float sd_spatula(float px_, float py_, float pz_) {  // object_spatula.hpp:40-82
+  const float halfWidth = 0.368f, halfLength = 0.736f, halfThickness = 0.07f, offset = 0.05f;
+  float px = fabsf(px_), py = pz_;
+  float b1 = halfWidth + offset, b2 = (halfWidth + offset) * 0.25f, he = halfLength + offset;
+  float bax = b2 - b1, bay = he - (-he);
+  float pax = px - b1, pay = py - (-he);
+  float h = fmaxf(0.f, fminf(1.f, (pax * bax + pay * bay) / (bax * bax + bay * bay)));
+  float dxs = pax - bax * h, dys = pay - bay * h;
+  float d_side = sqrtf(dxs * dxs + dys * dys);
+  float inside_x = b1 - (b1 - b2) * (py + he) / (2.f * he);
+  float d_inside = px - inside_x;
+  float d2 = (px < inside_x) ? d_inside : d_side;
+  if (py > he) {
+    d2 = sqrtf(px * px + (py - he) * (py - he)) - b2;
+  } else if (py < -he) {
+    float rx = halfWidth + offset, rz = 1.5f * (halfWidth + offset);
+    float qx = px, qz = py + he;
+    float k0 = sqrtf((qx / rx) * (qx / rx) + (qz / rz) * (qz / rz));
+    float k1 = sqrtf((qx / (rx * rx)) * (qx / (rx * rx)) + (qz / (rz * rz)) * (qz / (rz * rz)));
+    d2 = k0 * (k0 - 1.f) / k1;
+  }
+  float dy = fabsf(py_) - halfThickness;
+  float mx = fmaxf(d2, dy);
+  float ex = fmaxf(d2, 0.f), ey = fmaxf(dy, 0.f);
+  return fminf(mx, 0.f) + sqrtf(ex * ex + ey * ey);
+}
+__device__ float sd_box(const ObjDev& o, float px, float py, float pz) {
+  float qx = fabsf(px) - o.half[0], qy = fabsf(py) - o.half[1], qz = fabsf(pz) - o.half[2];
+  float ox = fmaxf(qx, 0.f), oy = fmaxf(qy, 0.f), oz = fmaxf(qz, 0.f);
+  return sqrtf(ox * ox + oy * oy + oz * oz) + fminf(fmaxf(qx, fmaxf(qy, qz)), 0.f);
+}
+__device__ __forceinline__ float sd_local(const ObjDev& o, float x, float y, float z) {
+  return o.kind == OBJ_SPATULA ? sd_spatula(x, y, z) : sd_box(o, x, y, z);
+}
+__device__ __forceinline__ void to_local(const ObjDev& o, const float X[3], float p[3]) {
+  float a = X[0] - o.tx, b = X[1] - o.ty, d = X[2] - o.tz;
+  p[0] = o.Rinv[0] * a + o.Rinv[1] * b + o.Rinv[2] * d;
+  p[1] = o.Rinv[3] * a + o.Rinv[4] * b + o.Rinv[5] * d;
+  p[2] = o.Rinv[6] * a + o.Rinv[7] * b + o.Rinv[8] * d;
+}
+__device__ bool obj_inside(const ObjDev& o, const float X[3]) {
+  if (o.kind == OBJ_GROUND) return !(X[1] > o.y0);
+  if (o.kind == OBJ_CURVE) return !(X[1] > X[0] * X[0]);
+  float p[3];
+  to_local(o, X, p);
+  return sd_local(o, p[0], p[1], p[2]) < 0.f;
+}
+__device__ void obj_normal(const ObjDev& o, const float X[3], float n[3]) {
+  if (o.kind == OBJ_GROUND) { n[0] = 0.f; n[1] = 1.f; n[2] = 0.f; return; }
+  if (o.kind == OBJ_CURVE) {
+    float a = -2.f * X[0], b = 1.f;
+    float l = sqrtf(a * a + b * b);
+    n[0] = a / l; n[1] = b / l; n[2] = 0.f;
+    return;
+  }
+  float p[3];
+  to_local(o, X, p);
+  const float e = 1e-4f;  // object_spatula.hpp:109-117
+  float nl[3] = {sd_local(o, p[0] + e, p[1], p[2]) - sd_local(o, p[0] - e, p[1], p[2]),
+                 sd_local(o, p[0], p[1] + e, p[2]) - sd_local(o, p[0], p[1] - e, p[2]),
+                 sd_local(o, p[0], p[1], p[2] + e) - sd_local(o, p[0], p[1], p[2] - e)};
+  float l = sqrtf(nl[0] * nl[0] + nl[1] * nl[1] + nl[2] * nl[2]);
+  if (l > 0.f) { nl[0] /= l; nl[1] /= l; nl[2] /= l; }
+  // (linear^-1)^T n = Rinv^T n
+  float w[3] = {o.Rinv[0] * nl[0] + o.Rinv[3] * nl[1] + o.Rinv[6] * nl[2],
+                o.Rinv[1] * nl[0] + o.Rinv[4] * nl[1] + o.Rinv[7] * nl[2],
+                o.Rinv[2] * nl[0] + o.Rinv[5] * nl[1] + o.Rinv[8] * nl[2]};
+  float wl = sqrtf(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  if (wl > 0.f) { w[0] /= wl; w[1] /= wl; w[2] /= wl; }
+  n[0] = w[0]; n[1] = w[1]; n[2] = w[2];
+}
+__device__ void obj_velocity(const ObjDev& o, const float X[3], float v[3]) {
+  if (o.kind == OBJ_GROUND || o.kind == OBJ_CURVE) { v[0] = v[1] = v[2] = 0.f; return; }
+  float r[3] = {X[0] - o.tx, X[1] - o.ty, X[2] - o.tz};
+  v[0] = o.vlin[0] + (o.omega[1] * r[2] - o.omega[2] * r[1]);
+  v[1] = o.vlin[1] + (o.omega[2] * r[0] - o.omega[0] * r[2]);
+  v[2] = o.vlin[2] + (o.omega[0] * r[1] - o.omega[1] * r[0]);
+}
+__device__ bool plate_inside(const PlateDev& pl, const float X[3]) {  // object_plate.hpp:13-57
+  switch (pl.type) {
+    case PT_LEFT: return X[1] < pl.upper && X[1] > pl.lower && (X[0] - pl.pos) <= 0;
+    case PT_RIGHT: return X[1] < pl.upper && X[1] > pl.lower && (pl.pos - X[0]) <= 0;
+    case PT_BOTTOM: return X[0] < pl.upper && X[0] > pl.lower && (X[1] - pl.pos) <= 0;
+    case PT_TOP: return X[0] < pl.upper && X[0] > pl.lower && (pl.pos - X[1]) <= 0;
+    case PT_BACK: return X[2] - pl.pos <= 0;
+    case PT_FRONT: return pl.pos - X[2] <= 0;
+  }
+  return false;
+}
+
+// boundary_collision.cpp:5-316 (3D branch)
+__device__ void boundary_collision(const Ctrl* c, float dtf, float dx, float Xi_[3], float vi[3], uint32_t& err) {
+  float vo[3] = {vi[0], vi[1], vi[2]};
+  float Xi[3] = {Xi_[0] + dtf * vi[0], Xi_[1] + dtf * vi[1], Xi_[2] + dtf * vi[2]};
+  bool infl = false;
+  const int knife = c->knife;
+  if (knife >= 0) {
+    const ObjDev& o = c->objects[knife];
+    float p[3];
+    to_local(o, Xi, p);
+    if (sd_local(o, p[0], p[1], p[2]) < 2.f * dx) infl = true;
+  }
+  for (int oi = 0; oi < c->n_objects; ++oi) {
+    const ObjDev& o = c->objects[oi];
+    if (!obj_inside(o, Xi)) continue;
+    float vobj[3];
+    obj_velocity(o, Xi, vobj);
+    float vr[3] = {vo[0] - vobj[0], vo[1] - vobj[1], vo[2] - vobj[2]};
+    if (o.bc == BC_NOSLIP) { vr[0] = vr[1] = vr[2] = 0.f; }
+    else if (o.bc == BC_SLIPFREE) {
+      float n[3];
+      obj_normal(o, Xi, n);
+      float dot = vr[0] * n[0] + vr[1] * n[1] + vr[2] * n[2];
+      if (dot < 0.f) {
+        float vt[3] = {vr[0] - dot * n[0], vr[1] - dot * n[1], vr[2] - dot * n[2]};
+        if (o.friction > 0.f) {
+          float vtn = sqrtf(vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]);
+          if (-dot * o.friction < vtn) { float sc = dot * o.friction / vtn; for (int k = 0; k < 3; ++k) vr[k] = vt[k] + vt[k] * sc; }
+          else { vr[0] = vr[1] = vr[2] = 0.f; }
+        } else { vr[0] = vt[0]; vr[1] = vt[1]; vr[2] = vt[2]; }
+      }
+    } else if (o.bc == BC_SLIPSTICK) {
+      float n[3];
+      obj_normal(o, Xi, n);
+      float dot = vr[0] * n[0] + vr[1] * n[1] + vr[2] * n[2];
+      for (int k = 0; k < 3; ++k) vr[k] -= dot * n[k];
+      if (dot < 0.f && o.friction > 0.f) {
+        float vtn = sqrtf(vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]);
+        if (-dot * o.friction < vtn) { float sc = dot * o.friction / vtn; for (int k = 0; k < 3; ++k) vr[k] += vr[k] * sc; }
+        else { vr[0] = vr[1] = vr[2] = 0.f; }
+      }
+    } else { err |= E_INVALID_BC; return; }
+    for (int k = 0; k < 3; ++k) vi[k] = vr[k] + vobj[k];
+    if (oi == knife) {
+      infl = true;
+      if (Xi[1] < 0.8f * dx) {  // thin-film rule, boundary_collision.cpp:93-111
+        float n[3];
+        obj_normal(o, Xi, n);
+        float t[3] = {-n[1] * n[0], 1.f - n[1] * n[1], -n[1] * n[2]};
+        float tn = sqrtf(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        if (tn > 1e-6f) { t[0] /= tn; t[1] /= tn; t[2] /= tn; } else { t[0] = t[1] = t[2] = 0.f; }
+        float vn = sqrtf(vobj[0] * vobj[0] + vobj[1] * vobj[1] + vobj[2] * vobj[2]);
+        for (int k = 0; k < 3; ++k) vi[k] = vobj[k] + t[k] * (0.2f * vn);
+      }
+    }
+    vo[0] = vi[0]; vo[1] = vi[1]; vo[2] = vi[2];
+  }
+  for (int pi = 0; pi < c->n_plates; ++pi) {
+    const PlateDev& pl = c->plates[pi];
+    if (!plate_inside(pl, Xi)) continue;
+    if (infl && pl.type == PT_BOTTOM) {
+      if (vi[1] < pl.vy) { vi[1] = pl.vy; vo[0] = vi[0]; vo[1] = vi[1]; vo[2] = vi[2]; }
+      continue;
+    }
+    float vr[3] = {vo[0] - pl.vx, vo[1] - pl.vy, vo[2] - pl.vz};
+    const int nax = (pl.type == PT_TOP || pl.type == PT_BOTTOM) ? 1 : (pl.type == PT_LEFT || pl.type == PT_RIGHT) ? 0 : 2;
+    const int t0 = nax == 0 ? 1 : 0, t1 = nax == 2 ? 1 : 2;
+    bool apply;
+    if (pl.bc == BC_NOSLIP) { vr[0] = vr[1] = vr[2] = 0.f; apply = false; }
+    else if (pl.bc == BC_SLIPSTICK) apply = true;
+    else if (pl.bc == BC_SLIPFREE) {
+      apply = (pl.type == PT_TOP && vr[1] > 0) || (pl.type == PT_BOTTOM && vr[1] < 0) ||
+              (pl.type == PT_LEFT && vr[0] < 0) || (pl.type == PT_RIGHT && vr[0] > 0) ||
+              (pl.type == PT_FRONT && vr[2] > 0) || (pl.type == PT_BACK && vr[2] < 0);
+    } else { err |= E_INVALID_BC; return; }
+    if (apply) {
+      float vel_t = sqrtf(vr[t0] * vr[t0] + vr[t1] * vr[t1]);
+      float fvn = pl.friction * fabsf(vr[nax]);
+      if (pl.friction == 0.f) {
+      } else if (vel_t <= fvn) { vr[t0] = 0.f; vr[t1] = 0.f; }
+      else { float sc = (vel_t - fvn) / vel_t; vr[t0] *= sc; vr[t1] *= sc; }
+      vr[nax] = 0.f;
+    }
+    vi[0] = vr[0] + pl.vx; vi[1] = vr[1] + pl.vy; vi[2] = vr[2] + pl.vz;
+    vo[0] = vi[0]; vo[1] = vi[1]; vo[2] = vi[2];
+  }
+}
+
+__global__ void k_grid_update(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  const int nn = c->n_nodes;
+  const float dtf = (float)c->dt;
+  const float dtv = dtf * P.particle_volume;
+  const float dtg[3] = {dtf * P.gravity[0], dtf * P.gravity[1], dtf * P.gravity[2]};
+  const int stride = gridDim.x * blockDim.x;
+  uint32_t err = 0;
+  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += stride) {
+    if (P.use_musl) B.gmusl[n] = z;
+    float4* rec = B.grid + (size_t)n * 4;
+    float4 r0 = rec[0];
+    if (!(r0.x > 0.f)) continue;
+    float4 r1 = rec[1], r2 = rec[2], r3 = rec[3];
+    const float sw = r0.x;
+    const float inv = 1.f / sw;
+    // P2G normalisation (p2g.cpp:97-124)
+    float v[3] = {r0.y * inv, r0.z * inv, r0.w * inv};
+    float lat[7] = {r1.w * inv, r2.x * inv, r2.y * inv, r2.z * inv, r2.w * inv, r3.x * inv, r3.y * inv};
+    float shear = r3.z * inv;
+    float ps = lat[0] + lat[1] + lat[2] + lat[3];
+    if (ps > 1e-6f) { for (int k = 0; k < 4; ++k) lat[k] /= ps; }
+    const float mi = sw * P.particle_mass;
+    // explicit update (explicit_euler_update.cpp:199-229)
+    float nv[3];
+    const float fs = -dtv / mi;
+    nv[0] = v[0] + (r1.x * fs + dtg[0]);
+    nv[1] = v[1] + (r1.y * fs + dtg[1]);
+    nv[2] = v[2] + (r1.z * fs + dtg[2]);
+    // node position
+    const int b = n >> 6, loc = n & 63;
+    int bx, by, bz;
+    brick_coords(b, c, bx, by, bz);
+    const int gi[3] = {c->g0[0] + bx * 4 + (loc >> 4), c->g0[1] + by * 4 + ((loc >> 2) & 3), c->g0[2] + bz * 4 + (loc & 3)};
+    float X[3] = {node_pos(gi[0], P.anchor[0], P.dx), node_pos(gi[1], P.anchor[1], P.dx), node_pos(gi[2], P.anchor[2], P.dx)};
+    boundary_collision(c, dtf, P.dx, X, nv, err);
+    rec[0] = make_float4(mi, nv[0], nv[1], nv[2]);
+    rec[1] = make_float4(nv[0] - v[0], nv[1] - v[1], nv[2] - v[2], lat[0]);
+    rec[2] = make_float4(lat[1], lat[2], lat[3], lat[4]);
+    rec[3] = make_float4(lat[5], lat[6], shear, 0.f);
+  }
+  if (err) atomicOr(&B.ctrl->error_flags, err);
+}
+
+// ------------------------------------------------------------------------------------------
+// G2P + mixing + MUSL (velocity update and re-scatter)
+// ------------------------------------------------------------------------------------------
+constexpr int kG2PCh = 14;  // v3 flip3 lat7 shear1
+struct __align__(16) StageMUSL {
+  float N[9];
+  float q[3];
+  float Cc[9];
+  float pad[3];
+};
+static_assert(sizeof(StageMUSL) == 24 * 4, "stage size");
+
+size_t g2p_smem_bytes() {
+  return sizeof(float) * (kG2PCh + 4) * kTileNodes + sizeof(StageMUSL) * kThreads;
+}
+
+__device__ __forceinline__ float smooth_step(float e0, float e1, float x) {  // g2p.cpp:7-10
+  float t = fmaxf(0.f, fminf(1.f, (x - e0) / (e1 - e0)));
+  return t * t * (3.f - 2.f * t);
+}
+
+__global__ void __launch_bounds__(kThreads) k_g2p_musl(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* tile = reinterpret_cast<float*>(smem_raw);     // [14][216]
+  float* mtile = tile + kG2PCh * kTileNodes;             // [4][216]
+  StageMUSL* st = reinterpret_cast<StageMUSL*>(mtile + 4 * kTileNodes);
+  const int S = P.np_stride;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int la = lane / 9, lb = (lane / 3) % 3, lc = lane % 3;
+  const float D = P.apicD, dx = P.dx;
+  const float fr = P.flip_ratio;
+  const bool apic = fr < 0.f, use_flip = fr >= -1.f, musl = P.use_musl != 0;
+  const float dtf = (float)c->dt;
+  // pigment mixing factor pieces (g2p.cpp:105-119)
+  float time_factor = 1.f;
+  {
+    float ct = (float)c->time;
+    if (ct > P.start_boost && P.end_boost > P.start_boost) {
+      float t = (ct - P.start_boost) / (P.end_boost - P.start_boost);
+      t = fminf(fmaxf(t, 0.f), 1.f);
+      time_factor = 1.f + t * (P.boost_factor - 1.f);
+    }
+  }
+  const float dyn = P.D_max * time_factor;
+  const int nbr = c->n_bricks;
+  for (int b = blockIdx.x; b < nbr; b += gridDim.x) {
+    const uint32_t* cs = B.cell + (size_t)b * kBrickNodes;
+    const uint32_t ps = cs[0], pe = cs[kBrickNodes];
+    if (ps == pe) continue;
+    int bx, by, bz;
+    brick_coords(b, c, bx, by, bz);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kTileNodes * 4; i += kThreads) {
+      const int tn = i >> 2, part = i & 3;
+      const int node = tile_to_node(tn, bx, by, bz, c);
+      float4 r = node >= 0 ? B.grid[(size_t)node * 4 + part] : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (part == 0) { tile[0 * kTileNodes + tn] = r.y; tile[1 * kTileNodes + tn] = r.z; tile[2 * kTileNodes + tn] = r.w; }
+      else if (part == 1) { tile[3 * kTileNodes + tn] = r.x; tile[4 * kTileNodes + tn] = r.y; tile[5 * kTileNodes + tn] = r.z; tile[6 * kTileNodes + tn] = r.w; }
+      else if (part == 2) { tile[7 * kTileNodes + tn] = r.x; tile[8 * kTileNodes + tn] = r.y; tile[9 * kTileNodes + tn] = r.z; tile[10 * kTileNodes + tn] = r.w; }
+      else { tile[11 * kTileNodes + tn] = r.x; tile[12 * kTileNodes + tn] = r.y; tile[13 * kTileNodes + tn] = r.z; }
+    }
+    for (int i = threadIdx.x; i < 4 * kTileNodes; i += kThreads) mtile[i] = 0.f;
+    for (uint32_t c0 = ps; c0 < pe; c0 += kThreads) {
+      const uint32_t c1 = min(c0 + (uint32_t)kThreads, pe);
+      __syncthreads();
+      if (c0 + threadIdx.x < c1) {
+        const uint32_t i = c0 + threadIdx.x;
+        const uint32_t o = B.sorted[i];
+        float xp[3], vold[3], lat[7];
+        AxisW aw[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          xp[d] = B.pin[(F_X + d) * S + o];
+          vold[d] = B.pin[(F_V + d) * S + o];
+          aw[d] = axis_weights(xp[d], P.anchor[d], dx, P.inv_dx);
+        }
+#pragma unroll
+        for (int k = 0; k < 7; ++k) lat[k] = B.pin[(F_LAT + k) * S + o];
+        // local cell of the particle within the tile
+        // local cell of the particle in its brick (always 0..3 by construction; clamped so a
+        // particle outside the step's box can never index past the tile)
+        const int lx = min(max(aw[0].base - c->g0[0] - bx * 4, 0), 3);
+        const int ly = min(max(aw[1].base - c->g0[1] - by * 4, 0), 3);
+        const int lz = min(max(aw[2].base - c->g0[2] - bz * 4, 0), 3);
+        float vp[3] = {0.f, 0.f, 0.f}, fp[3] = {0.f, 0.f, 0.f}, Bp[9], L[9], gl[7], gs = 0.f;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { Bp[k] = 0.f; L[k] = 0.f; }
+#pragma unroll
+        for (int k = 0; k < 7; ++k) gl[k] = 0.f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const float dxa = (float)a * dx - aw[0].r;
+#pragma unroll
+          for (int bb = 0; bb < 3; ++bb) {
+            const float dyb = (float)bb * dx - aw[1].r;
+            const float nxy = aw[0].N[a] * aw[1].N[bb];
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+              const float dzc = (float)cc * dx - aw[2].r;
+              const int tn = ((lx + a) * kTile + (ly + bb)) * kTile + (lz + cc);
+              const float w = nxy * aw[2].N[cc];
+              const float g[3] = {aw[0].dN[a] * aw[1].N[bb] * aw[2].N[cc], aw[0].N[a] * aw[1].dN[bb] * aw[2].N[cc],
+                                  nxy * aw[2].dN[cc]};
+              const float gv[3] = {tile[tn], tile[kTileNodes + tn], tile[2 * kTileNodes + tn]};
+#pragma unroll
+              for (int r = 0; r < 3; ++r) {
+                vp[r] += gv[r] * w;
+                const float wv = gv[r] * w;
+                Bp[3 * r + 0] += wv * dxa;
+                Bp[3 * r + 1] += wv * dyb;
+                Bp[3 * r + 2] += wv * dzc;
+                L[3 * r + 0] += gv[r] * g[0];
+                L[3 * r + 1] += gv[r] * g[1];
+                L[3 * r + 2] += gv[r] * g[2];
+                fp[r] += tile[(3 + r) * kTileNodes + tn] * w;
+              }
+#pragma unroll
+              for (int k = 0; k < 7; ++k) gl[k] += tile[(6 + k) * kTileNodes + tn] * w;
+              gs += tile[13 * kTileNodes + tn] * w;
+            }
+          }
+        }
+        if (!apic) for (int k = 0; k < 9; ++k) Bp[k] = 0.f;
+        if (!use_flip) { fp[0] = fp[1] = fp[2] = 0.f; }
+        // diffusion factor |0.5 (L + L^T)|_F (g2p.cpp:98-101)
+        float s2 = 0.f;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int q = 0; q < 3; ++q) { float sv = 0.5f * (L[3 * r + q] + L[3 * q + r]); s2 += sv * sv; }
+        const float diff = sqrtf(s2);
+        // mixing (g2p.cpp:105-130)
+        const float mixf = smooth_step(P.D_edge0, P.D_edge1, gs);
+        const float smix = fminf(fmaxf(dyn * mixf * dtf, 0.f), 1.f);
+#pragma unroll
+        for (int k = 0; k < 7; ++k) lat[k] = (1.f - smix) * lat[k] + smix * gl[k];
+        const float psum = lat[0] + lat[1] + lat[2] + lat[3];
+        if (psum > 1e-6f) { for (int k = 0; k < 4; ++k) lat[k] /= psum; }
+        // MUSL velocity update (musl.cpp:13-26)
+        float vnew[3];
+        if (musl) {
+          for (int r = 0; r < 3; ++r) {
+            if (fr < -1.f) vnew[r] = vp[r];
+            else if (fr < 0.f) vnew[r] = (-fr) * (vold[r] + fp[r]) + (1.f - (-fr)) * vp[r];
+            else vnew[r] = fr * (vold[r] + fp[r]) + (1.f - fr) * vp[r];
+          }
+        } else {
+          for (int r = 0; r < 3; ++r) vnew[r] = vold[r];
+          for (int r = 0; r < 3; ++r) B.pic[(3 + r) * S + i] = fp[r];
+        }
+        float* po = B.pout;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) { po[(F_V + r) * S + i] = vnew[r]; B.pic[r * S + i] = vp[r]; }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) po[(F_B + k) * S + i] = Bp[k];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) po[(F_LAT + k) * S + i] = lat[k];
+        po[F_DIFF * S + i] = diff;
+        if (musl) {
+          StageMUSL& s = st[threadIdx.x];
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) s.N[3 * d + k] = aw[d].N[k];
+          const float r3[3] = {aw[0].r, aw[1].r, aw[2].r};
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            float Br = Bp[3 * q] * r3[0] + Bp[3 * q + 1] * r3[1] + Bp[3 * q + 2] * r3[2];
+            s.q[q] = vnew[q] - D * Br;
+          }
+#pragma unroll
+          for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) s.Cc[3 * k + q] = D * dx * Bp[3 * q + k];
+        }
+      }
+      __syncthreads();
+      if (musl) {
+        for (int cl = warp; cl < kBrickNodes; cl += kWarps) {
+          const uint32_t s0 = max(cs[cl], c0), s1 = min(cs[cl + 1], c1);
+          if (s0 >= s1 || lane >= 27) continue;
+          float acc[4] = {0.f, 0.f, 0.f, 0.f};
+          const float fa = (float)la, fb = (float)lb, fc = (float)lc;
+          for (uint32_t sp = s0; sp < s1; ++sp) {
+            const StageMUSL& s = st[sp - c0];
+            const float w = s.N[la] * s.N[3 + lb] * s.N[6 + lc];
+            const float wm = w > 1e-25f ? w : 0.f;  // musl.cpp:188
+#pragma unroll
+            for (int q = 0; q < 3; ++q) acc[q] += wm * (s.q[q] + fa * s.Cc[q] + fb * s.Cc[3 + q] + fc * s.Cc[6 + q]);
+            acc[3] += wm;
+          }
+          const int lx = cl >> 4, ly = (cl >> 2) & 3, lz = cl & 3;
+          const int tn = ((lx + la) * kTile + (ly + lb)) * kTile + (lz + lc);
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (acc[k] != 0.f) atomicAdd(&mtile[k * kTileNodes + tn], acc[k]);
+        }
+      }
+    }
+    __syncthreads();
+    if (musl) {
+      for (int tn = threadIdx.x; tn < kTileNodes; tn += kThreads) {
+        const float w = mtile[3 * kTileNodes + tn];
+        if (w == 0.f) continue;
+        const int node = tile_to_node(tn, bx, by, bz, c);
+        if (node < 0) continue;
+        red_add_v4(B.gmusl + node, mtile[tn], mtile[kTileNodes + tn], mtile[2 * kTileNodes + tn], w);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// FP64 3x3 SVD (one-sided Jacobi, Hestenes) -- sigma >= 0, U, V orthogonal
+// ------------------------------------------------------------------------------------------
+__device__ void svd3_d(const double A[9], double U[9], double s[3], double V[9]) {
+  double W[9];
+  for (int k = 0; k < 9; ++k) W[k] = A[k];
+  V[0] = 1; V[1] = 0; V[2] = 0; V[3] = 0; V[4] = 1; V[5] = 0; V[6] = 0; V[7] = 0; V[8] = 1;
+  const double eps = 2.220446049250313e-16;
+  for (int sweep = 0; sweep < 12; ++sweep) {
+    bool rotated = false;
+#pragma unroll
+    for (int pq = 0; pq < 3; ++pq) {
+      const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
+      double alpha = W[p] * W[p] + W[3 + p] * W[3 + p] + W[6 + p] * W[6 + p];
+      double beta = W[q] * W[q] + W[3 + q] * W[3 + q] + W[6 + q] * W[6 + q];
+      double gamma = W[p] * W[q] + W[3 + p] * W[3 + q] + W[6 + p] * W[6 + q];
+      if (gamma == 0.0 || fabs(gamma) <= eps * sqrt(alpha * beta)) continue;
+      rotated = true;
+      double zeta = (beta - alpha) / (2.0 * gamma);
+      double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+      double cs = rsqrt(1.0 + t * t);
+      double sn = cs * t;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double wp = W[3 * k + p], wq = W[3 * k + q];
+        W[3 * k + p] = cs * wp - sn * wq;
+        W[3 * k + q] = sn * wp + cs * wq;
+        double vp = V[3 * k + p], vq = V[3 * k + q];
+        V[3 * k + p] = cs * vp - sn * vq;
+        V[3 * k + q] = sn * vp + cs * vq;
+      }
+    }
+    if (!rotated) break;
+  }
+  int valid = 0;
+  for (int j = 0; j < 3; ++j) {
+    s[j] = sqrt(W[j] * W[j] + W[3 + j] * W[3 + j] + W[6 + j] * W[6 + j]);
+  }
+  // left vectors; a column with zero norm is completed from the others
+  int zero_cols = 0;
+  int zc = -1;
+  for (int j = 0; j < 3; ++j) {
+    if (s[j] > 1e-300) {
+      double inv = 1.0 / s[j];
+      for (int k = 0; k < 3; ++k) U[3 * k + j] = W[3 * k + j] * inv;
+      ++valid;
+    } else { ++zero_cols; zc = j; }
+  }
+  if (zero_cols == 1) {
+    int a = (zc + 1) % 3, b = (zc + 2) % 3;
+    U[0 + zc] = U[3 + a] * U[6 + b] - U[6 + a] * U[3 + b];
+    U[3 + zc] = U[6 + a] * U[0 + b] - U[0 + a] * U[6 + b];
+    U[6 + zc] = U[0 + a] * U[3 + b] - U[3 + a] * U[0 + b];
+  } else if (zero_cols > 1) {
+    for (int k = 0; k < 9; ++k) U[k] = (k % 4 == 0) ? 1.0 : 0.0;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// deformation update + return map + position update + stress cache + reductions
+// ------------------------------------------------------------------------------------------
+struct ReturnMapOut {
+  double h[3];       // final principal log strains
+  bool changed;      // F replaced by U exp(h) V^T
+  bool to_rotation;  // capped VM branch: F = U V^T
+};
+
+// plasticity.cpp:163-238 (VMVisc) and :240-340 (DPVisc) in FP64
+__device__ void return_map(const Params& P, double dt, const double sg[3], float& epd, float& epv, float& epp, float& dgam,
+                           uint32_t& plastic, uint32_t& err, ReturnMapOut& out) {
+  double h[3];
+  for (int i = 0; i < 3; ++i) h[i] = log(fmax(fabs(sg[i]), 1e-4));
+  const double htr = h[0] + h[1] + h[2];
+  double hd[3] = {h[0] - htr / 3.0, h[1] - htr / 3.0, h[2] - htr / 3.0};
+  const double hdn = sqrt(hd[0] * hd[0] + hd[1] * hd[1] + hd[2] * hd[2]);
+  if (hdn > 0) for (int i = 0; i < 3; ++i) hd[i] /= hdn;
+  out.changed = false;
+  out.to_rotation = false;
+  for (int i = 0; i < 3; ++i) out.h[i] = h[i];
+  const double fmu = P.f_mu_prefac, emu = P.e_mu_prefac, dpre = P.d_prefac;
+  if (P.plastic_model == PL_VMVISC) {
+    const double q_trial = emu * hdn;
+    double q_yield = P.q_min + (P.q_max - P.q_min) * exp(-P.xi * (double)epd);
+    const double p_trial = -P.K * htr;
+    if (p_trial < P.p_min * exp(-P.xi * (double)epv)) {
+      double dg = q_trial / fmu;
+      out.to_rotation = true;
+      out.changed = true;
+      epv = (float)((double)epv + (-p_trial / P.K));
+      epd = (float)((double)epd + dg / dpre);
+      dgam = (float)(dg / dt);
+    } else if (q_trial > q_yield) {
+      ++plastic;
+      double dg;
+      if (P.perzyna_exp == 1.0 && P.xi == 0.0) {
+        dg = (q_trial - q_yield) / (fmu + q_yield * P.perzyna_visc / dt);
+        if (dg < 0) err |= E_NEG_DGAMMA;
+      } else {
+        dg = 0.01 * (q_trial - q_yield) / fmu;
+        for (int it = 0; it < 60; ++it) {
+          if (it == 59) err |= E_NEWTON_NOCONV;
+          double tm = P.perzyna_visc * dg + dt;
+          double tmp = dt / tm;
+          double tmp1 = pow(tmp, P.perzyna_exp);
+          q_yield = P.q_min + (P.q_max - P.q_min) * exp(-P.xi * ((double)epd + dg / dpre));
+          double res = (q_trial - fmu * dg) * tmp1 - q_yield;
+          if (fabs(res) < 1e-2) break;
+          double qyd = -P.xi / dpre * (P.q_max - P.q_min) * exp(-P.xi * ((double)epd + dg / dpre));
+          double rd = -fmu * tmp1 + (q_trial - fmu * dg) * P.perzyna_exp * pow(tmp, P.perzyna_exp - 1.0) *
+                                        (-P.perzyna_visc * dt) / (tm * tm) - qyd;
+          if (fabs(rd) < 1e-14) err |= E_NEWTON_FLAT;
+          dg -= res / rd;
+          if (dg < 0) dg = 1e-10;
+        }
+      }
+      for (int i = 0; i < 3; ++i) out.h[i] = h[i] - (dg / dpre) * hd[i];
+      out.changed = true;
+      epd = (float)((double)epd + dg / dpre);
+      dgam = (float)(dg / dt);
+    }
+  } else if (P.plastic_model == PL_DPVISC) {
+    const double p_trial = -P.K * htr;
+    const double q_trial = emu * hdn;
+    const double p_tip = -P.q_cohesion / P.M;
+    const double p_shift = P.use_pradhana ? -P.K * (double)epp : 0.0;
+    const double q_yield = P.M * (p_trial + p_shift) + P.q_cohesion;
+    if ((p_trial + p_shift) < p_tip) {
+      const double dg = dpre * hdn;
+      const double epv_inst = (p_tip - p_trial) / P.K;
+      ++plastic;
+      const double hh = -p_tip / (P.K * 3.0);
+      for (int i = 0; i < 3; ++i) out.h[i] = hh;
+      out.changed = true;
+      dgam = (float)(dg / dt);
+      epd = (float)((double)epd + dg / dpre);
+      epv = (float)((double)epv + epv_inst);
+      if (P.use_pradhana) epp = (float)((double)epp + epv_inst);
+    } else {
+      if (P.use_pradhana) epp = 0.f;
+      dgam = 0.f;
+    }
+    if ((p_trial + p_shift) > p_tip && q_trial > q_yield) {
+      ++plastic;
+      double dg;
+      if (P.perzyna_exp == 1.0) {
+        dg = (q_trial - q_yield) / (fmu + q_yield * P.perzyna_visc / dt);
+        if (dg < 0) err |= E_NEG_DGAMMA;
+      } else {
+        dg = 0.01 * (q_trial - q_yield) / fmu;
+        for (int it = 0; it < 60; ++it) {
+          if (it == 59) err |= E_NEWTON_NOCONV;
+          double tm = P.perzyna_visc * dg + dt;
+          double tmp = dt / tm;
+          double tmp1 = pow(tmp, P.perzyna_exp);
+          double res = (q_trial - fmu * dg) * tmp1 - q_yield;
+          if (fabs(res) < 1e-2) break;
+          double rd = -fmu * tmp1 + (q_trial - fmu * dg) * P.perzyna_exp * pow(tmp, P.perzyna_exp - 1.0) *
+                                        (-P.perzyna_visc * dt) / (tm * tm);
+          if (fabs(rd) < 1e-14) err |= E_NEWTON_FLAT;
+          dg -= res / rd;
+          if (dg < 0) dg = 1e-10;
+        }
+      }
+      for (int i = 0; i < 3; ++i) out.h[i] = h[i] - (dg / dpre) * hd[i];
+      out.changed = true;
+      epd = (float)((double)epd + dg / dpre);
+      dgam = (float)(dg / dt);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_defgrad(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  const int S = P.np_stride, np = P.np;
+  const double dt = c->dt;
+  const float dtf = (float)dt;
+  const float dx = P.dx;
+  uint32_t err = 0, plastic = 0, nact = 0;
+  float maxv2 = 0.f;
+  int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+  const int stride = gridDim.x * blockDim.x;
+  const float fr = P.flip_ratio;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
+    const uint32_t o = B.sorted[i];
+    const uint32_t meta = B.meta_in[o];
+    float* po = B.pout;
+    const float* pi = B.pin;
+    if (meta & kInactiveBit) {  // carried through unchanged (G2P zeroes B, deformation update zeroes delta_gamma)
+      for (int f = 0; f < F_COUNT; ++f) {
+        float v = pi[f * S + o];
+        if ((f >= F_B && f < F_B + 9) || f == F_DG) v = 0.f;
+        po[f * S + i] = v;
+      }
+      B.meta_out[i] = meta;
+      continue;
+    }
+    float xp[3];
+    AxisW aw[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      xp[d] = pi[(F_X + d) * S + o];
+      aw[d] = axis_weights(xp[d], P.anchor[d], dx, P.inv_dx);
+    }
+    // node indices of the stencil per axis
+    int bidx[3][3], lidx[3][3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        int n = min(max(aw[d].base + k - c->g0[d], 0), c->dims[d] - 1);  // inside the box by construction
+        bidx[d][k] = n >> 2;
+        lidx[d][k] = n & 3;
+      }
+    // velocity gradient from the MUSL grid (deformation_update.cpp:26-39)
+    float L[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) L[k] = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const int node = ((bidx[0][a] * c->nb[1] + bidx[1][bb]) * c->nb[2] + bidx[2][cc]) * kBrickNodes +
+                           lidx[0][a] * 16 + lidx[1][bb] * 4 + lidx[2][cc];
+          float gv[3];
+          if (P.use_musl) {
+            const float4 m = B.gmusl[node];
+            const float inv = m.w > 0.f ? 1.f / m.w : 0.f;
+            gv[0] = m.x * inv; gv[1] = m.y * inv; gv[2] = m.z * inv;
+          } else {
+            const float4 m = B.grid[(size_t)node * 4];
+            gv[0] = m.y; gv[1] = m.z; gv[2] = m.w;
+          }
+          const float g[3] = {aw[0].dN[a] * aw[1].N[bb] * aw[2].N[cc], aw[0].N[a] * aw[1].dN[bb] * aw[2].N[cc],
+                              aw[0].N[a] * aw[1].N[bb] * aw[2].dN[cc]};
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) L[3 * r + q] += gv[r] * g[q];
+        }
+    // F_trial = F + dt L F (FP64)
+    double F[9], Ft[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) F[k] = (double)pi[(F_F + k) * S + o];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s += (double)L[3 * r + k] * F[3 * k + q];
+        Ft[3 * r + q] = F[3 * r + q] + dt * s;
+      }
+    float epd = pi[F_EPD * S + o], epv = pi[F_EPV * S + o], epp = pi[F_EPP * S + o], dgam = 0.f;
+    double U[9], V[9], sg[3];
+    svd3_d(Ft, U, sg, V);
+    double hfin[3];
+    float Fout[9];
+    bool changed = false;
+    if (P.plastic_model != PL_NONE) {
+      ReturnMapOut rm;
+      return_map(P, dt, sg, epd, epv, epp, dgam, plastic, err, rm);
+      changed = rm.changed;
+      if (rm.to_rotation) { hfin[0] = hfin[1] = hfin[2] = 0.0; }
+      else for (int k = 0; k < 3; ++k) hfin[k] = rm.h[k];
+    }
+    if (changed) {
+      double e[3] = {exp(hfin[0]), exp(hfin[1]), exp(hfin[2])};
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+          Fout[3 * r + q] = (float)(U[3 * r] * e[0] * V[3 * q] + U[3 * r + 1] * e[1] * V[3 * q + 1] + U[3 * r + 2] * e[2] * V[3 * q + 2]);
+    } else {
+      for (int k = 0; k < 3; ++k) hfin[k] = log(fabs(sg[k]));
+#pragma unroll
+      for (int k = 0; k < 9; ++k) Fout[k] = (float)Ft[k];
+    }
+    // Kirchhoff stress of the final F: tau = U diag(2 mu h + lambda tr h) U^T (simulation.hpp:287-294)
+    float tau[6];
+    {
+      const double tr = hfin[0] + hfin[1] + hfin[2];
+      double d[3];
+      for (int k = 0; k < 3; ++k) d[k] = 2.0 * P.mu * hfin[k] + P.lambda * tr;
+      if (!(isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2]))) { d[0] = d[1] = d[2] = 0.0; }
+      auto T = [&](int r, int q) { return U[3 * r] * d[0] * U[3 * q] + U[3 * r + 1] * d[1] * U[3 * q + 1] + U[3 * r + 2] * d[2] * U[3 * q + 2]; };
+      tau[0] = (float)T(0, 0); tau[1] = (float)T(1, 1); tau[2] = (float)T(2, 2);
+      tau[3] = (float)T(0, 1); tau[4] = (float)T(0, 2); tau[5] = (float)T(1, 2);
+    }
+    // position update (position_update.cpp:6-91)
+    float pic[3], v[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) { pic[r] = B.pic[r * S + i]; v[r] = po[(F_V + r) * S + i]; }
+    if (!P.use_musl) {
+      for (int r = 0; r < 3; ++r) {
+        const float fl = B.pic[(3 + r) * S + i];
+        if (fr < -1.f) v[r] = pic[r];
+        else if (fr < 0.f) v[r] = (-fr) * (v[r] + fl) + (1.f - (-fr)) * pic[r];
+        else v[r] = fr * (v[r] + fl) + (1.f - fr) * pic[r];
+      }
+    }
+    float xn[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) xn[r] = xp[r] + dtf * pic[r];
+    bool active = true;
+    bool bad = false;
+    for (int r = 0; r < 3; ++r)
+      if (isnan(xn[r]) || isinf(xn[r]) || isnan(v[r]) || isinf(v[r])) bad = true;
+    if (bad) {
+      active = false;
+      err |= E_NAN_PARTICLE;
+      for (int r = 0; r < 3; ++r) { v[r] = 0.f; xn[r] = P.use_particle_boundaries ? P.pbmin[r] : 0.f; }
+    } else {
+      if (xn[1] < 0.f) { xn[1] = 0.f; if (v[1] < 0.f) v[1] = 0.f; }
+      if (P.use_particle_boundaries) {
+        for (int r = 0; r < 3; ++r) {
+          if (xn[r] < P.pbmin[r]) { xn[r] = P.pbmin[r]; active = false; v[r] = 0.f; }
+          else if (xn[r] > P.pbmax[r]) { xn[r] = P.pbmax[r]; active = false; v[r] = 0.f; }
+        }
+        if (!active) v[0] = v[1] = v[2] = 0.f;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) { po[(F_X + r) * S + i] = xn[r]; po[(F_V + r) * S + i] = v[r]; }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = Fout[k];
+    po[F_EPD * S + i] = epd; po[F_EPV * S + i] = epv; po[F_EPP * S + i] = epp; po[F_DG * S + i] = dgam;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) po[(F_TAU + k) * S + i] = tau[k];
+    B.meta_out[i] = active ? meta : (meta | kInactiveBit);
+    if (active) {
+      ++nact;
+      maxv2 = fmaxf(maxv2, v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      for (int r = 0; r < 3; ++r) { int k = fkey(xn[r]); mn[r] = min(mn[r], k); mx[r] = max(mx[r], k); }
+    }
+  }
+  // block reduction, then one set of atomics per block
+  __shared__ int red_i[kWarps][8];
+  __shared__ uint32_t red_u[kWarps][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t mv = __reduce_max_sync(0xffffffffu, __float_as_uint(maxv2));
+  uint32_t na = __reduce_add_sync(0xffffffffu, nact);
+  uint32_t pc = __reduce_add_sync(0xffffffffu, plastic);
+  uint32_t er = __reduce_or_sync(0xffffffffu, err);
+  int r6[6];
+  for (int r = 0; r < 3; ++r) { r6[r] = __reduce_min_sync(0xffffffffu, mn[r]); r6[3 + r] = __reduce_max_sync(0xffffffffu, mx[r]); }
+  if (lane == 0) {
+    red_u[warp][0] = mv; red_u[warp][1] = na; red_u[warp][2] = pc; red_u[warp][3] = er;
+    for (int k = 0; k < 6; ++k) red_i[warp][k] = r6[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kWarps; ++w) {
+      red_u[0][0] = max(red_u[0][0], red_u[w][0]);
+      red_u[0][1] += red_u[w][1];
+      red_u[0][2] += red_u[w][2];
+      red_u[0][3] |= red_u[w][3];
+      for (int r = 0; r < 3; ++r) { red_i[0][r] = min(red_i[0][r], red_i[w][r]); red_i[0][3 + r] = max(red_i[0][3 + r], red_i[w][3 + r]); }
+    }
+    Ctrl* cw = B.ctrl;
+    if (red_u[0][1]) {
+      atomicMax(&cw->max_v2, red_u[0][0]);
+      atomicAdd(&cw->n_active, red_u[0][1]);
+      for (int r = 0; r < 3; ++r) { atomicMin(&cw->xmin_key[r], red_i[0][r]); atomicMax(&cw->xmax_key[r], red_i[0][3 + r]); }
+    }
+    if (red_u[0][2]) atomicAdd(&cw->plastic_count, red_u[0][2]);
+    if (red_u[0][3]) atomicOr(&cw->error_flags, red_u[0][3]);
+  }
+}
+
+// Reductions over the current particle state (prepare time): max |v|^2, AABB, active count.
+__global__ void __launch_bounds__(kThreads) k_reduce_state(Params P, const float* pcur, const uint32_t* meta, Ctrl* cw) {
+  const int S = P.np_stride;
+  uint32_t nact = 0;
+  float maxv2 = 0.f;
+  int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.np; i += gridDim.x * blockDim.x) {
+    if (meta[i] & kInactiveBit) continue;
+    ++nact;
+    float v2 = 0.f;
+    for (int r = 0; r < 3; ++r) {
+      float v = pcur[(F_V + r) * S + i];
+      v2 += v * v;
+      int k = fkey(pcur[(F_X + r) * S + i]);
+      mn[r] = min(mn[r], k); mx[r] = max(mx[r], k);
+    }
+    maxv2 = fmaxf(maxv2, v2);
+  }
+  uint32_t mv = __reduce_max_sync(0xffffffffu, __float_as_uint(maxv2));
+  uint32_t na = __reduce_add_sync(0xffffffffu, nact);
+  int r6[6];
+  for (int r = 0; r < 3; ++r) { r6[r] = __reduce_min_sync(0xffffffffu, mn[r]); r6[3 + r] = __reduce_max_sync(0xffffffffu, mx[r]); }
+  if ((threadIdx.x & 31) == 0 && na) {
+    atomicMax(&cw->max_v2, mv);
+    atomicAdd(&cw->n_active, na);
+    for (int r = 0; r < 3; ++r) { atomicMin(&cw->xmin_key[r], r6[r]); atomicMax(&cw->xmax_key[r], r6[3 + r]); }
+  }
+}
+
+// Copy particle fields back to the original order: out[f][pid] = cur[f][i].
+__global__ void k_unpermute(Params P, const float* pcur, const uint32_t* meta, float* out, uint8_t* active_out) {
+  const int S = P.np_stride, np = P.np;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    const uint32_t m = meta[i];
+    const uint32_t pid = m & ~kInactiveBit;
+    if (pid >= (uint32_t)np) continue;
+    for (int f = 0; f < F_COUNT; ++f) out[(size_t)f * np + pid] = pcur[f * S + i];
+    active_out[pid] = (m & kInactiveBit) ? 0 : 1;
+  }
+}
+
+// Diagnostics: mass, momentum, mass-weighted latent sums (double atomics per block).
+__global__ void __launch_bounds__(kThreads) k_stats(Params P, const float* pcur, const uint32_t* meta, double* acc) {
+  const int S = P.np_stride;
+  double s[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.np; i += gridDim.x * blockDim.x) {
+    if (meta[i] & kInactiveBit) continue;
+    s[0] += 1.0;
+    for (int r = 0; r < 3; ++r) s[1 + r] += pcur[(F_V + r) * S + i];
+    for (int k = 0; k < 7; ++k) s[4 + k] += pcur[(F_LAT + k) * S + i];
+  }
+  for (int k = 0; k < 11; ++k) {
+    double v = s[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&acc[k], v);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// host-side launchers
+// ------------------------------------------------------------------------------------------
+static int g_num_sms = 0;
+static int g_occ_p2g = 1, g_occ_g2p = 1, g_occ_def = 1;
+
+cudaError_t launch_init(int device) {
+  cudaError_t e = cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem_bytes());
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_g2p_musl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes());
+  if (e != cudaSuccess) return e;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_p2g, k_p2g, kThreads, p2g_smem_bytes());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_g2p, k_g2p_musl, kThreads, g2p_smem_bytes());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_def, k_defgrad, kThreads, 0);
+  if (g_occ_p2g < 1) g_occ_p2g = 1;
+  if (g_occ_g2p < 1) g_occ_g2p = 1;
+  if (g_occ_def < 1) g_occ_def = 1;
+  return cudaGetLastError();
+}
+
+int num_sms() { return g_num_sms; }
+
+void launch_step(const Params& P, const Bufs& B, cudaStream_t s) {
+  const int sms = g_num_sms > 0 ? g_num_sms : 148;
+  const int flat_grid = sms * 8;
+  k_prologue<<<1, 32, 0, s>>>(P, B);
+  k_clear<<<flat_grid, 256, 0, s>>>(P, B);
+  k_count<<<flat_grid, 256, 0, s>>>(P, B);
+  const int scan_blocks = (P.node_cap + 1 + kScanBlock - 1) / kScanBlock;
+  k_scan_local<<<scan_blocks, kScanThreads, 0, s>>>(P, B);
+  k_scan_top<<<1, kScanThreads, 0, s>>>(P, B);
+  k_scan_add<<<scan_blocks, kScanThreads, 0, s>>>(P, B);
+  k_scatter<<<flat_grid, 256, 0, s>>>(P, B);
+  k_p2g<<<sms * g_occ_p2g, kThreads, p2g_smem_bytes(), s>>>(P, B);
+  k_grid_update<<<flat_grid, 256, 0, s>>>(P, B);
+  k_g2p_musl<<<sms * g_occ_g2p, kThreads, g2p_smem_bytes(), s>>>(P, B);
+  k_defgrad<<<sms * g_occ_def, kThreads, 0, s>>>(P, B);
+  k_epilogue<<<1, 32, 0, s>>>(P, B);
+}
+
+int kernels_per_step() { return 12; }
+
+void launch_reduce_state(const Params& P, const float* pcur, const uint32_t* meta, Ctrl* ctrl, cudaStream_t s) {
+  const int sms = g_num_sms > 0 ? g_num_sms : 148;
+  k_reduce_state<<<sms * 4, kThreads, 0, s>>>(P, pcur, meta, ctrl);
+}
+void launch_unpermute(const Params& P, const float* pcur, const uint32_t* meta, float* out, uint8_t* active,
+                      cudaStream_t s) {
+  const int sms = g_num_sms > 0 ? g_num_sms : 148;
+  k_unpermute<<<sms * 4, 256, 0, s>>>(P, pcur, meta, out, active);
+}
+void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, double* acc, cudaStream_t s) {
+  const int sms = g_num_sms > 0 ? g_num_sms : 148;
+  k_stats<<<sms * 2, kThreads, 0, s>>>(P, pcur, meta, acc);
+}
+
+}  // namespace pm

@@ -1,0 +1,154 @@
+"""Seeded synthetic palette scenes (the workloads the step is measured and checked on).
+
+The reference builds its paint scene from OpenVDB blob level sets with Poisson-disk sampling
+(matter/src/simulation/simulation_blobs.cpp:7-150, 27 particles per cell); those assets and
+libraries are not used here.  These builders place cuboid paint blocks of 8 jittered particles
+per cell instead (2 x 2 x 2 sub-cells, uniform jitter inside each), all from a seed.
+
+A scene is a plain dict that ``apply(scene, sim)`` loads into any object with the Simulation
+call surface (the product :class:`Simulation` or the CPU oracle).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+# Mixbox latents (rgb -> 7-float latent: 4 pigment concentrations + 3 RGB residuals) of the scene
+# colours, as computed by Mixbox's float_rgb_to_latent for these sRGB triples.
+MIXBOX_LATENTS = {
+    (0.99, 0.86, 0.08): [0.003921568393707275, 0.8289437890052795, 0.0, 0.16713464260101318,
+                         0.02399754524230957, 0.03179413080215454, -0.01334661990404129],
+    (0.10, 0.20, 0.60): [0.7396079301834106, 0.02299606241285801, 0.07450980693101883, 0.16288620233535767,
+                         0.0012317672371864319, -0.0003674924373626709, -0.0024244189262390137],
+    (0.80, 0.10, 0.12): [0.002337253885343671, 0.0262086670845747, 0.8995293974876404, 0.07192468643188477,
+                         0.003439664840698242, -0.0034313425421714783, 0.0016628801822662354],
+    (0.05, 0.45, 0.25): [0.5207844376564026, 0.42559564113616943, 0.0, 0.05361992120742798,
+                         -0.03620488569140434, 0.015082001686096191, 0.0036397576332092285],
+}
+
+RGB_SEEDS = list(MIXBOX_LATENTS)
+
+# pigment_config.json of the reference (matter/pigment_config.json)
+PIGMENT_CONFIG = dict(pigment_D_max=50.0, pigment_D_edge0=1.5, pigment_D_edge1=7.0, start_boost_time=15.0,
+                      end_boost_time=30.0, boost_factor=3.0)
+
+
+def jittered_block(lo, ncells, dx, rng, per_axis=2):
+    """Particles at per_axis^3 sub-cells of every cell of a box, uniformly jittered inside each."""
+    n = np.asarray(ncells, dtype=np.int64)
+    sub = dx / per_axis
+    idx = np.stack(np.meshgrid(*[np.arange(k * per_axis) for k in n], indexing="ij"), -1).reshape(-1, 3)
+    return (np.asarray(lo, np.float64) + (idx + rng.uniform(0.0, 1.0, idx.shape)) * sub).astype(np.float32)
+
+
+def knife_path(rng, x_mid, y_c, z_lo, z_hi, segments=3, drift=0.1):
+    """A seeded piecewise-linear knife path sweeping back and forth through the paint along z."""
+    pts = []
+    for i in range(segments + 1):
+        z = z_lo if i % 2 == 0 else z_hi
+        pts.append([x_mid + rng.uniform(-drift, drift), y_c, z])
+    return np.asarray(pts, np.float64)
+
+
+def two_block_scene(dx: float, block_cells=(16, 16, 8), seed: int = 0, steps: int = 500, knife: bool = True,
+                    material: str = "vmvisc") -> dict:
+    """Two x-adjacent paint blocks resting on y = 0 in the unit cube, a box knife on a seeded
+    3-segment path at 0.5 units/s (friction 0.3), floor plate SlipStick with friction 1."""
+    rng = np.random.default_rng(seed)
+    bc = np.asarray(block_cells, np.int64)
+    size = bc * dx
+    x0 = 0.5 - size[0]
+    z0 = 0.5 - 0.5 * size[2]
+    a = jittered_block([x0, 0.0, z0], bc, dx, rng)
+    b = jittered_block([x0 + size[0], 0.0, z0], bc, dx, rng)
+    x = np.concatenate([a, b])
+    lat = np.concatenate([np.tile(MIXBOX_LATENTS[RGB_SEEDS[0]], (len(a), 1)),
+                          np.tile(MIXBOX_LATENTS[RGB_SEEDS[1]], (len(b), 1))]).astype(np.float32)
+    params = dict(rho=1300.0, E=5e4, nu=0.3, cfl=0.5, cfl_elastic=1.0, flip_ratio=-1.5, fps=60.0, end_frame=100000,
+                  dx=dx, particle_volume=dx ** 3 / 8.0, particle_mass=1300.0 * dx ** 3 / 8.0,
+                  use_particle_boundaries=1, q_prefac=1.0 / np.sqrt(2.0), **PIGMENT_CONFIG)
+    if material == "vmvisc":
+        # von Mises / Herschel-Bulkley: yield 100 Pa, consistency 10 Pa s^n, flow index 0.6.  The
+        # Perzyna residual q = q_y (1 + eta*gamma_dot)^n (plasticity.cpp:211) gives
+        # eta = (k / q_y)^(1/n).
+        params.update(plastic_model=5, q_max=100.0, q_min=100.0, xi=0.0, perzyna_exp=0.6,
+                      perzyna_visc=(10.0 / 100.0) ** (1.0 / 0.6))
+    elif material == "dpvisc":
+        # matter/sim_config.json: E 5e5, nu 0.2, rho 1000, friction angle 5 deg, cohesion 500,
+        # Perzyna exponent 1, viscosity 0.4; Pradhana correction on.
+        params.update(plastic_model=6, E=5e5, nu=0.2, rho=1000.0, particle_mass=1000.0 * dx ** 3 / 8.0,
+                      M=float(np.tan(np.deg2rad(5.0))), q_cohesion=500.0, perzyna_exp=1.0, perzyna_visc=0.4,
+                      use_pradhana=1)
+    vectors = dict(gravity=[0.0, -9.81, 0.0], grid_reference_point=[0.0, 0.0, 0.0],
+                   particle_boundary_min=[-2.0, -2.0, -2.0], particle_boundary_max=[2.0, 2.0, 2.0])
+    objects = [("plate", dict(pos=0.0, plate_type=1, bc=1, friction=1.0))]
+    if knife:
+        half = [0.2, 0.1, 0.005]
+        yk = half[1] + 0.5 * dx
+        path = knife_path(rng, 0.5, yk, z0 - 0.05, z0 + size[2] + 0.05)
+        objects.append(("box_knife", dict(bc=2, friction=0.3, half=half, waypoints=path, speed=0.5)))
+    return dict(x=x, latent=lat, params=params, vectors=vectors, objects=objects, steps=steps,
+                name=f"two_blocks_dx{1.0 / dx:.0f}")
+
+
+def config1(seed: int = 0) -> dict:
+    """64^3 grid, dx = 1/64, two 16x16x8-cell blocks: 32,768 particles, 500 steps."""
+    return two_block_scene(1.0 / 64, (16, 16, 8), seed, 500)
+
+
+def config2(seed: int = 0) -> dict:
+    """256^3 grid, dx = 1/256, two 64x64x32-cell blocks: 2,097,152 particles, 1000 steps."""
+    return two_block_scene(1.0 / 256, (64, 64, 32), seed, 1000)
+
+
+def four_block_scene(dx: float, block_cells=(64, 64, 64), seed: int = 0, steps: int = 2000) -> dict:
+    """2 x 2 blocks (in x and z) of four pigments on the floor, box knife through the middle."""
+    rng = np.random.default_rng(seed)
+    bc = np.asarray(block_cells, np.int64)
+    size = bc * dx
+    x0 = 0.5 - size[0]
+    z0 = 0.5 - size[2]
+    xs, lats = [], []
+    for k, (ix, iz) in enumerate([(0, 0), (1, 0), (0, 1), (1, 1)]):
+        blk = jittered_block([x0 + ix * size[0], 0.0, z0 + iz * size[2]], bc, dx, rng)
+        xs.append(blk)
+        lats.append(np.tile(MIXBOX_LATENTS[RGB_SEEDS[k]], (len(blk), 1)))
+    sc = two_block_scene(dx, block_cells, seed, steps)
+    sc["x"] = np.concatenate(xs)
+    sc["latent"] = np.concatenate(lats).astype(np.float32)
+    half = [0.2, 0.1, 0.005]
+    path = knife_path(rng, 0.5, half[1] + 0.5 * dx, z0 - 0.05, z0 + 2 * size[2] + 0.05)
+    sc["objects"] = [sc["objects"][0], ("box_knife", dict(bc=2, friction=0.3, half=half, waypoints=path, speed=0.5))]
+    sc["name"] = f"four_blocks_dx{1.0 / dx:.0f}"
+    return sc
+
+
+def config3(seed: int = 0) -> dict:
+    """384^3 grid, dx = 1/384, four 64^3-cell blocks of four pigments: 8,388,608 particles."""
+    return four_block_scene(1.0 / 384, (64, 64, 64), seed, 2000)
+
+
+def apply(scene: dict, sim) -> None:
+    """Load a scene into a Simulation-like object (product Simulation or the oracle wrapper)."""
+    if hasattr(sim, "setParticles"):  # product API
+        sim.setParticles(scene["x"], scene["latent"])
+        sim.set(**scene["params"])
+        for k, v in scene["vectors"].items():
+            setattr(sim, k, v)
+        for kind, kw in scene["objects"]:
+            if kind == "plate":
+                sim.addPlate(kw["pos"], kw["plate_type"], kw["bc"], kw["friction"])
+            elif kind == "box_knife":
+                sim.addBoxKnife(kw["bc"], kw["friction"], kw["half"], kw["waypoints"], kw["speed"])
+            elif kind == "spatula":
+                sim.addSpatula(kw["bc"], kw["friction"], frames=kw["frames"])
+    else:  # oracle wrapper
+        sim.set_particles(scene["x"], scene["latent"])
+        sim.set(**scene["params"])
+        sim.set(**scene["vectors"])
+        for kind, kw in scene["objects"]:
+            if kind == "plate":
+                sim.add_plate(kw["pos"], kw["plate_type"], kw["bc"], kw["friction"])
+            elif kind == "box_knife":
+                sim.add_box_knife(kw["bc"], kw["friction"], kw["half"], kw["waypoints"], kw["speed"])
+            elif kind == "spatula":
+                sim.add_spatula(kw["bc"], kw["friction"], kw["frames"])

@@ -1,0 +1,226 @@
+"""Python mirror of the reference ``Simulation`` class (matter/src/simulation/simulation.hpp:25-186)
+on top of the C ABI.  Method names follow the reference; public fields are properties that set
+the same-named parameters through ``pm_set_param``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from ._lib import call
+
+# matter/src/tools.hpp:55-59
+PLATE_TOP, PLATE_BOTTOM, PLATE_LEFT, PLATE_RIGHT, PLATE_FRONT, PLATE_BACK = range(6)
+BC_NOSLIP, BC_SLIPSTICK, BC_SLIPFREE = range(3)
+NO_PLASTICITY, VM, DP, DPSOFT, MCC, VMVISC, DPVISC, MCCVISC, DPMUI, MCCMUI = range(10)
+RETURN_MAP_PLAIN, RETURN_MAP_SURROGATE = 0, 1
+
+_SCALARS = ("cfl", "cfl_elastic", "flip_ratio", "rho", "E", "nu", "fps", "end_frame", "min_dt", "dx",
+            "particle_mass", "particle_volume", "plastic_model", "use_pradhana", "use_musl",
+            "use_particle_boundaries", "q_max", "q_min", "p_min", "M", "q_cohesion", "perzyna_exp",
+            "perzyna_visc", "xi", "q_prefac", "pigment_D_max", "pigment_D_edge0", "pigment_D_edge1",
+            "start_boost_time", "end_boost_time", "boost_factor", "auto_frame")
+_READONLY = ("time", "dt", "step", "Np", "mu", "lambda", "K", "dt_max", "frame_dt", "final_time",
+             "n_active", "plastic_count", "grid_nodes", "frame")
+_VECTORS = ("gravity", "particle_boundary_min", "particle_boundary_max", "grid_reference_point")
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _fp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Particles:
+    """Host copy of the particle state in the original particle order (data_structures.hpp:9-50)."""
+
+    def __init__(self, d: dict):
+        self.__dict__.update(d)
+
+
+class Simulation:
+    """One MPM scene on one GPU.  Mirrors ``Simulation`` (simulation.hpp:25-186)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        call("pm_create", device, C.byref(h))
+        self._h = h
+        self._np = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            call("pm_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- public fields ---------------------------------------------------------------------
+    def __getattr__(self, name):
+        if name.startswith("_"):
+            raise AttributeError(name)
+        if name in _SCALARS or name in _READONLY:
+            out = C.c_double()
+            call("pm_get_param", self._h, name.encode(), C.byref(out))
+            return out.value
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        if name.startswith("_"):
+            object.__setattr__(self, name, value)
+        elif name in _SCALARS or name == "frame":
+            call("pm_set_param", self._h, name.encode(), float(value))
+        elif name in _VECTORS:
+            v = np.ascontiguousarray(value, dtype=np.float64).reshape(3)
+            call("pm_set_param3", self._h, name.encode(), _dp(v))
+        else:
+            object.__setattr__(self, name, value)
+
+    def set(self, **kw) -> "Simulation":
+        for k, v in kw.items():
+            setattr(self, k, v)
+        return self
+
+    @property
+    def Np(self) -> int:
+        return self._np
+
+    # ---- reference API -----------------------------------------------------------------------
+    def initializeBasic(self, name: str) -> None:  # simulation_units.cpp:9-26
+        call("pm_initialize_basic", self._h, name.encode())
+
+    def loadPigmentConfig(self, path: str) -> None:  # simulation_units.cpp:31-48
+        call("pm_load_pigment_config", self._h, path.encode())
+
+    def loadSimConfig(self, path: str) -> None:  # simulation_units.cpp:50-80
+        call("pm_load_sim_config", self._h, path.encode())
+
+    def setParticles(self, x, latent=None, v=None) -> None:
+        x = _f32(x).reshape(-1, 3)
+        n = x.shape[0]
+        lat = None if latent is None else _f32(latent).reshape(n, 7)
+        vv = None if v is None else _f32(v).reshape(n, 3)
+        call("pm_set_particles", self._h, n, _fp(x), _fp(lat), _fp(vv))
+        self._np = n
+
+    def setupScene(self, fps: float, pigment_config: Optional[str] = None, sim_config: Optional[str] = None,
+                   anim_path: Optional[str] = None) -> None:  # simulation_units.cpp:28-131
+        enc = lambda s: None if s is None else s.encode()
+        call("pm_setup_scene", self._h, float(fps), enc(pigment_config), enc(sim_config), enc(anim_path))
+
+    def prepareSimulation(self) -> None:  # simulation_units.cpp:133-215
+        call("pm_prepare", self._h)
+
+    def step(self) -> None:  # simulation_units.cpp:217-233
+        call("pm_step", self._h)
+
+    def advance(self, nsteps: int) -> int:
+        """nsteps of step() + frameFinished() on the device; returns frames finished."""
+        fd = C.c_uint32()
+        call("pm_advance", self._h, int(nsteps), C.byref(fd))
+        return fd.value
+
+    def frameFinished(self) -> bool:  # simulation_units.cpp:235-241
+        o = C.c_int()
+        call("pm_frame_finished", self._h, C.byref(o))
+        return bool(o.value)
+
+    def isFinished(self) -> bool:  # simulation_units.cpp:243-245
+        o = C.c_int()
+        call("pm_is_finished", self._h, C.byref(o))
+        return bool(o.value)
+
+    def getGridBoundaries(self):  # simulation_units.cpp:247-255
+        lo, hi = np.zeros(3), np.zeros(3)
+        call("pm_get_grid_boundaries", self._h, _dp(lo), _dp(hi))
+        return lo, hi
+
+    def getSpatulaObject(self):  # simulation.hpp:186 as read in MPMIntegrationSim.cpp:144-167
+        ex = C.c_int()
+        inv, half = np.zeros(16), np.zeros(3)
+        call("pm_get_knife", self._h, C.byref(ex), _dp(inv), _dp(half))
+        if not ex.value:
+            return None
+        return inv.reshape(4, 4), half
+
+    # ---- objects -----------------------------------------------------------------------------
+    def addPlate(self, pos, plate_type, bc=BC_NOSLIP, friction=0.0, pos_lower=-1e15, pos_upper=1e15, vx=0.0,
+                 vy=0.0, vz=0.0, vmin_factor=1.0, load_factor=0.0) -> None:  # object_plate.hpp:13-28
+        call("pm_add_plate", self._h, float(pos), int(plate_type), int(bc), float(friction), float(pos_lower),
+             float(pos_upper), float(vx), float(vy), float(vz), float(vmin_factor), float(load_factor))
+
+    def addSpatula(self, bc, friction, frames=None, anim_path: Optional[str] = None) -> None:
+        if anim_path is not None:
+            call("pm_add_spatula_file", self._h, int(bc), float(friction), anim_path.encode())
+        else:
+            fr = _f32(frames).reshape(-1, 7)
+            call("pm_add_spatula", self._h, int(bc), float(friction), _fp(fr), fr.shape[0])
+
+    def addBoxKnife(self, bc, friction, half, waypoints, speed, quat_wxyz=None) -> None:
+        h = np.ascontiguousarray(half, dtype=np.float64)
+        w = np.ascontiguousarray(waypoints, dtype=np.float64).reshape(-1, 3)
+        q = None if quat_wxyz is None else np.ascontiguousarray(quat_wxyz, dtype=np.float64)
+        call("pm_add_box_knife", self._h, int(bc), float(friction), _dp(h), _dp(w), w.shape[0], float(speed), _dp(q))
+
+    def addGround(self, bc, friction, y0=0.0) -> None:  # object_ground.hpp:14
+        call("pm_add_ground", self._h, int(bc), float(friction), float(y0))
+
+    def addCurve(self, bc, friction) -> None:  # object_curve.hpp:13
+        call("pm_add_curve", self._h, int(bc), float(friction))
+
+    def setReturnMap(self, mode: int) -> None:
+        call("pm_set_return_map", self._h, int(mode))
+
+    # ---- readback ------------------------------------------------------------------------------
+    def getParticles(self, fields=("x", "v", "latent", "diffusion", "active")) -> Particles:
+        n = self._np
+        shapes = dict(x=(n, 3), v=(n, 3), latent=(n, 7), diffusion=(n,), F=(n, 3, 3), B=(n, 3, 3), plastic=(n, 4))
+        arrs = {k: np.zeros(shapes[k], np.float32) for k in shapes if k in fields}
+        act = np.zeros(n, np.uint8) if "active" in fields else None
+        call("pm_get_particles", self._h, _fp(arrs.get("x")), _fp(arrs.get("v")), _fp(arrs.get("latent")),
+             _fp(arrs.get("diffusion")), None if act is None else act.ctypes.data_as(C.POINTER(C.c_uint8)),
+             _fp(arrs.get("F")), _fp(arrs.get("B")), _fp(arrs.get("plastic")))
+        if act is not None:
+            arrs["active"] = act
+        return Particles(arrs)
+
+    @property
+    def particles(self) -> Particles:
+        return self.getParticles()
+
+    def errorFlags(self, clear: bool = False) -> int:
+        f = C.c_uint32()
+        call("pm_get_error_flags", self._h, C.byref(f), int(clear))
+        return f.value
+
+    def stats(self) -> dict:
+        m = C.c_double()
+        mom, lat = np.zeros(3), np.zeros(7)
+        na = C.c_uint32()
+        call("pm_get_stats", self._h, C.byref(m), _dp(mom), _dp(lat), C.byref(na))
+        return dict(mass=m.value, momentum=mom, mean_latent=lat, n_active=na.value)
+
+    def grid(self) -> dict:
+        origin = np.zeros(3)
+        dims = np.zeros(3, np.uint32)
+        call("pm_get_grid", self._h, _dp(origin), dims.ctypes.data_as(C.POINTER(C.c_uint32)), None, None, None, None,
+             None, None)
+        n = int(np.prod(dims.astype(np.int64)))
+        out = dict(origin=origin, dims=dims.astype(int), mass=np.zeros(n, np.float32),
+                   v_update=np.zeros((n, 3), np.float32), v_musl=np.zeros((n, 3), np.float32),
+                   flip=np.zeros((n, 3), np.float32), latent=np.zeros((n, 7), np.float32),
+                   shear=np.zeros(n, np.float32))
+        call("pm_get_grid", self._h, _dp(origin), dims.ctypes.data_as(C.POINTER(C.c_uint32)), _fp(out["mass"]),
+             _fp(out["v_update"]), _fp(out["v_musl"]), _fp(out["flip"]), _fp(out["latent"]), _fp(out["shear"]))
+        return out

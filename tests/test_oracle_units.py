@@ -1,0 +1,106 @@
+"""Unit tests of the CPU oracle's restated pieces (the checker must be right before it judges)."""
+import numpy as np
+import pytest
+
+
+def test_svd3_reconstructs_and_orders(oracle_mod):
+    rng = np.random.default_rng(3)
+    mats = [np.eye(3), np.diag([2.0, 0.5, 1.0]), np.diag([1.0, 1.0, -1.0]),
+            np.array([[1.0, 2.0, 0.0], [2.0, 4.0, 0.0], [0.0, 0.0, 1.0]])]  # rank 2
+    mats += [np.eye(3) + 0.5 * rng.standard_normal((3, 3)) for _ in range(50)]
+    for A in mats:
+        U, s, V = oracle_mod.svd3(A)
+        assert np.all(s >= 0) and s[0] >= s[1] >= s[2]
+        assert np.allclose(U @ np.diag(s) @ V.T, A, atol=1e-12)
+        assert np.allclose(U.T @ U, np.eye(3), atol=1e-12)
+        assert np.allclose(V.T @ V, np.eye(3), atol=1e-12)
+        assert np.allclose(s, np.linalg.svd(A, compute_uv=False), atol=1e-12)
+
+
+def test_svd_function_of_sigma_is_convention_free(oracle_mod):
+    """U g(S) V^T equals R g(P) of the polar decomposition for any SVD with sigma >= 0 -- the
+    property that makes the return map independent of Eigen's JacobiSVD conventions."""
+    rng = np.random.default_rng(4)
+    for _ in range(20):
+        A = np.eye(3) + 0.3 * rng.standard_normal((3, 3))
+        U, s, V = oracle_mod.svd3(A)
+        Un, sn, Vtn = np.linalg.svd(A)
+        g = lambda x: np.exp(0.5 * np.log(np.maximum(x, 1e-4)))
+        assert np.allclose(U @ np.diag(g(s)) @ V.T, Un @ np.diag(g(sn)) @ Vtn, atol=1e-12)
+
+
+def test_spatula_sdf_shape(oracle_mod):
+    """object_spatula.hpp:40-82: extruded trapezoid, half thickness 0.07, symmetric in x and y."""
+    sd = oracle_mod.sd_spatula
+    assert sd([0, 0, 0]) == pytest.approx(-0.07)
+    assert sd([0, 0.07, 0]) == pytest.approx(0.0, abs=1e-12)
+    assert sd([0, 0.17, 0]) == pytest.approx(0.1, abs=1e-12)
+    for p in ([0.1, 0.02, 0.3], [0.2, -0.03, -0.5], [0.05, 0.1, 0.9]):
+        q = [-p[0], p[1], p[2]]
+        r = [p[0], -p[1], p[2]]
+        assert sd(p) == pytest.approx(sd(q)) and sd(p) == pytest.approx(sd(r))
+    assert sd([3.0, 0.0, 0.0]) > 2.0
+
+
+def test_slerp_endpoints_and_norm(oracle_mod):
+    rng = np.random.default_rng(5)
+    for _ in range(20):
+        a = rng.standard_normal(4); a /= np.linalg.norm(a)
+        b = rng.standard_normal(4); b /= np.linalg.norm(b)
+        assert np.allclose(oracle_mod.slerp(a, b, 0.0), a)
+        e = oracle_mod.slerp(a, b, 1.0)
+        assert np.allclose(e, b if a @ b >= 0 else -b)
+        for t in (0.25, 0.5, 0.8):
+            assert np.linalg.norm(oracle_mod.slerp(a, b, t)) == pytest.approx(1.0, abs=1e-12)
+
+
+def _small_scene(oracle_mod, material="vmvisc", steps=1):
+    from pigment_mixing_b200 import scenes
+    sc = scenes.two_block_scene(1.0 / 32, (8, 8, 4), seed=1, steps=steps, material=material)
+    o = oracle_mod.OracleSim(64)
+    o.set(n_threads=4)
+    scenes.apply(sc, o)
+    o.prepare()
+    return sc, o
+
+
+def test_mass_and_momentum_conservation(oracle_mod):
+    """simulation.cpp:302-348: grid mass equals particle mass and grid momentum equals particle
+    momentum to 1e-10 (relative) -- here for the MUSL grid of the last step."""
+    sc, o = _small_scene(oracle_mod)
+    o.advance(3)
+    g = o.grid()
+    p = o.particles_f64()
+    mp = sc["params"]["particle_mass"]
+    assert g["mass"].astype(np.float64).sum() == pytest.approx(mp * len(sc["x"]), rel=1e-6)
+    mom_grid = (g["mass"][:, None].astype(np.float64) * g["v"].astype(np.float64)).sum(0)
+    mom_part = mp * p["v"].sum(0)
+    assert np.allclose(mom_grid, mom_part, rtol=1e-5, atol=1e-9 * np.abs(mom_part).max() + 1e-12)
+
+
+def test_latent_concentrations_stay_normalised(oracle_mod):
+    """g2p.cpp:125-130: after mixing the four concentrations sum to one."""
+    sc, o = _small_scene(oracle_mod)
+    o.advance(10)
+    lat = o.particles_f64()["latent"]
+    assert np.allclose(lat[:, :4].sum(1), 1.0, atol=1e-12)
+
+
+def test_vmvisc_projection_is_consistent(oracle_mod):
+    """plasticity.cpp:163-238: after projection q = q_y (1 + eta * delta_gamma)^m on every
+    plastic particle (the Perzyna consistency condition, Newton tolerance 1e-2 Pa)."""
+    sc, o = _small_scene(oracle_mod)
+    o.advance(15)
+    p = o.particles()
+    prm = sc["params"]
+    mu = prm["E"] / (2 * (1 + prm["nu"]))
+    dg = p["plastic"][:, 3].astype(np.float64)
+    idx = np.nonzero(dg > 0)[0]
+    assert len(idx) > 0
+    for i in idx[:200]:
+        s = np.linalg.svd(p["F"][i].astype(np.float64), compute_uv=False)
+        h = np.log(np.maximum(s, 1e-4))
+        dev = h - h.mean()
+        q = 2 * prm["q_prefac"] * mu * np.linalg.norm(dev)
+        target = prm["q_max"] * (1 + prm["perzyna_visc"] * dg[i]) ** prm["perzyna_exp"]
+        assert q == pytest.approx(target, rel=2e-3, abs=0.05)
