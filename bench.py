@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Throughput of the paint-mixing MPM step (particle-steps/s) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload 2m|8m|32k]
+
+Workload (default "2m"): two 64x64x32-cell paint blocks at dx = 1/256 (2,097,152 particles,
+8 jittered particles per cell, seeded), von Mises / Herschel-Bulkley viscoplastic paint
+(yield 100 Pa, 10 Pa s^0.6), box knife on a seeded 3-segment path at 0.5 units/s, floor plate,
+MUSL, FP32 transfers with FP64 SVD/return map.  A "step" is one MPM time step of that scene.
+
+``value`` is device-timed (CUDA events on the library's stream, state resident in HBM);
+``e2e`` is the same metric through the C ABI from pinned host buffers: scene upload, prepare,
+K steps with the particle readback at every finished frame (the render loop's idiom), and the
+final readback, timed on the host clock.  Multi-GPU runs are independent replicas (one scene per
+GPU, no collective on the data path): value sums over ranks, time is the max over ranks.
+``--impl reference`` times the CPU restatement of the reference step (the oracle, float,
+-O3 -ffast-math -fopenmp, all host threads) on the same scene.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s"
+# Algorithmic bytes per unit of work (per particle, per active grid node) of each kernel: the
+# compulsory SoA particle traffic and grid traffic of the reference step structure.
+ALGO_BYTES = {
+    "k_p2g": (128.0, 48.0),          # read x,v,B,latent,diffusion,tau ; accumulate m,mv,f,latent,shear
+    "k_g2p_musl": (144.0, 108.0),    # read x,v,latent + write v,B,latent,diff,pic ; read grid + MUSL grid
+    "k_defgrad": (136.0, 12.0),      # read x,pic,F,plastic + write x,F,plastic ; read MUSL velocity
+    "k_grid_update": (0.0, 40.0),    # read 16 B, write v and flip 24 B per node
+    "k_clear": (0.0, 48.0),          # zero the accumulated record
+}
+STEP_BYTES = (408.0, 256.0)          # whole step: 408 B per particle + 256 B per active node
+
+
+def _workload(name: str):
+    from pigment_mixing_b200 import scenes
+    if name == "2m":
+        return scenes.config2(seed=0)
+    if name == "8m":
+        return scenes.config3(seed=0)
+    if name == "32k":
+        return scenes.config1(seed=0)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return None, 0, 1, 0
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=None)
+    return dist, rank, ws, local
+
+
+def _max_over_ranks(dist, x: float, device) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist, device):
+    if dist is not None:
+        import torch
+        t = torch.zeros(1, device=device)
+        dist.all_reduce(t)
+        torch.cuda.synchronize(device)
+
+
+def cpu_baseline(scene, budget_s: float = 25.0, max_steps: int = 20):
+    """The oracle (float, -O3 -ffast-math -fopenmp, all host threads) on the same scene."""
+    from oracle.oracle import OracleSim
+    from pigment_mixing_b200 import scenes
+    cores = os.cpu_count() or 1
+    o = OracleSim(32, fast=True)
+    o.set(n_threads=cores)
+    scenes.apply(scene, o)
+    o.prepare()
+    t0 = time.perf_counter()
+    o.advance(1)  # first step allocates
+    first = time.perf_counter() - t0
+    n = int(max(1, min(max_steps, budget_s / max(first, 1e-3))))
+    t0 = time.perf_counter()
+    o.advance(n)
+    el = time.perf_counter() - t0
+    npart = len(scene["x"])
+    return {"value": npart * n / el, "unit": METRIC, "cores": cores, "kind": "port",
+            "sample": f"{n} full steps of the {npart}-particle scene after 1 warm-up step "
+                      f"(CPU restatement of the reference step, float, OpenMP)", "seconds": el}
+
+
+def run_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return  # replicas: rank 0 alone times the CPU path
+    scene = _workload(args.workload)
+    b = cpu_baseline(scene, budget_s=max(10.0, min(120.0, 3.0 * args.steps)), max_steps=max(1, args.steps))
+    line = {"impl": "reference", "metric": METRIC, "value": b["value"], "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": len(scene["x"]) / b["value"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": _config(scene, args),
+            "cpu_baseline": {k: b[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": b["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _config(scene, args):
+    n = len(scene["x"])
+    return {"workload": f"{scene['name']}: {n} particles, dx={scene['params']['dx']:.6g}, two cuboid paint blocks, "
+                        "VMVisc (Herschel-Bulkley) paint, box knife 0.4x0.2x0.01 on a 3-segment path at 0.5 u/s, "
+                        "MUSL, APIC",
+            "particles": n, "return_map": args.return_map,
+            "precision": "FP32 transfers and grid, FP64 SVD and return map",
+            "l2": "inputs larger than L2 (particle state 0.35 GB per buffer at 2M particles)",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+def run_ours(args):
+    import torch
+    from pigment_mixing_b200 import Simulation, scenes
+    dist, rank, ws, local = _dist()
+    device = local
+    torch.cuda.set_device(device)
+    scene = _workload(args.workload)
+    npart = len(scene["x"])
+    sim = Simulation(device)
+    scenes.apply(scene, sim)
+    sim.prepareSimulation()
+    sim.advance(args.warmup)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=device)
+    # -------- timed region: K steps, state resident in HBM --------
+    with ClockSampler(device) as clk:
+        _barrier(dist, device)
+        torch.cuda.synchronize(device)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        sim.advance(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize(device)
+        ms = ev0.elapsed_time(ev1)
+        _barrier(dist, device)
+    clocks = clk.summary()
+    flags = sim.errorFlags()
+    ms_max = _max_over_ranks(dist, ms, device)
+    value = ws * npart * args.steps / (ms_max / 1e3)
+    # -------- per-kernel times (CUDA events on the same stream, separate steps) --------
+    g = sim.grid()
+    active_nodes = int((g["mass"] > 0).sum())
+    kps = int(sim.kernels_per_step)
+    kms = sim.profileSteps(5)
+    dom = max((k for k in kms if k in ALGO_BYTES), key=lambda k: kms[k])
+    peak, peak_kind = _peaks()
+    pb, nb = ALGO_BYTES[dom]
+    algo = pb * npart + nb * active_nodes
+    achieved = algo / (kms[dom] / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_2m.json")
+    if args.workload == "2m" and os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get(dom)
+        except Exception:
+            traffic = None
+    step_ms = ms_max / args.steps
+    step_bytes = STEP_BYTES[0] * npart + STEP_BYTES[1] * active_nodes
+    roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": algo,
+            "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"}
+    step_roof = {"bytes": step_bytes, "achieved": step_bytes / (step_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                 "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak, "active_nodes": active_nodes}
+    sim.close()
+    # -------- end to end through the C ABI from pinned host buffers --------
+    e2e = _e2e(scene, args, device, dist, ws)
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": _config(scene, args),
+            "roofline": roof, "step_roofline": step_roof, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": args.steps * kps,
+            "kernel_ms": kms, "error_flags": flags}
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        line["cpu_baseline"] = {k: v for k, v in cpu_baseline(scene).items() if k != "seconds"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def _e2e(scene, args, device, dist, ws):
+    import torch
+    from pigment_mixing_b200 import Simulation, scenes
+    n = len(scene["x"])
+    hx = torch.from_numpy(np.ascontiguousarray(scene["x"], np.float32)).pin_memory()
+    hl = torch.from_numpy(np.ascontiguousarray(scene["latent"], np.float32)).pin_memory()
+    ox = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    ol = torch.empty((n, 7), dtype=torch.float32).pin_memory()
+    od = torch.empty((n,), dtype=torch.float32).pin_memory()
+    _barrier(dist, device)
+    t0 = time.perf_counter()
+    sim = Simulation(device)
+    sim.setParticles(hx.numpy(), hl.numpy())
+    sim.set(**scene["params"])
+    for k, v in scene["vectors"].items():
+        setattr(sim, k, v)
+    for kind, kw in scene["objects"]:
+        if kind == "plate":
+            sim.addPlate(kw["pos"], kw["plate_type"], kw["bc"], kw["friction"])
+        elif kind == "box_knife":
+            sim.addBoxKnife(kw["bc"], kw["friction"], kw["half"], kw["waypoints"], kw["speed"])
+    sim.prepareSimulation()
+    frames = 0
+    done = 0
+    chunk = 16
+    while done < args.steps:
+        k = min(chunk, args.steps - done)
+        if sim.advance(k) > 0:
+            sim.readInto(x=ox.numpy(), latent=ol.numpy(), diffusion=od.numpy())
+            frames += 1
+        done += k
+    sim.readInto(x=ox.numpy(), latent=ol.numpy(), diffusion=od.numpy())
+    el = time.perf_counter() - t0
+    sim.close()
+    el_max = _max_over_ranks(dist, el, device)
+    h2d = (hx.numel() + hl.numel()) * 4
+    d2h = (frames + 1) * (ox.numel() + ol.numel() + od.numel()) * 4
+    return {"value": ws * n * args.steps / el_max, "unit": METRIC, "h2d_bytes_per_step": h2d / args.steps,
+            "d2h_bytes_per_step": d2h / args.steps, "frames_read_back": frames + 1,
+            "includes": "upload, prepare, K steps, per-frame x/latent/diffusion readback"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="2m", choices=["2m", "8m", "32k"])
+    ap.add_argument("--return-map", default="plain", choices=["plain"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -76,7 +76,7 @@ PM_API pm_status pm_initialize_basic(pm_sim* sim, const char* name);
  * "perzyna_visc", "xi", "q_prefac", "pigment_D_max", "pigment_D_edge0", "pigment_D_edge1",
  * "start_boost_time", "end_boost_time", "boost_factor", "frame", "auto_frame".
  * Read-only extras for pm_get_param: "time", "dt", "step", "Np", "mu", "lambda", "K", "dt_max",
- * "frame_dt", "final_time", "n_active", "plastic_count", "grid_nodes". */
+ * "frame_dt", "final_time", "n_active", "plastic_count", "grid_nodes", "kernels_per_step". */
 PM_API pm_status pm_set_param(pm_sim* sim, const char* name, double value);
 PM_API pm_status pm_get_param(pm_sim* sim, const char* name, double* value);
 /* Vector fields: "gravity", "particle_boundary_min", "particle_boundary_max", "grid_reference_point". */
@@ -161,6 +161,17 @@ PM_API pm_status pm_get_grid(pm_sim* sim, double origin[3], uint32_t dims[3], fl
 /* ---- learned return map (no reference counterpart) ----------------------------------------- */
 /* Selects the return-map implementation used by pm_step/pm_advance. */
 PM_API pm_status pm_set_return_map(pm_sim* sim, int mode);
+
+/* ---- diagnostics (no reference counterpart; the reference times phases with gettimeofday,
+ * simulation.cpp:247-274) -------------------------------------------------------------------- */
+/* The cudaStream_t all of this simulation's work is issued on (for CUDA event timing). */
+PM_API pm_status pm_get_stream(pm_sim* sim, void** stream);
+/* Name of the i-th kernel of a step (launch order), "" when out of range. */
+PM_API const char* pm_kernel_name(int index);
+/* Runs nsteps ordinary steps (no graph), timing every kernel with CUDA events on the stream;
+ * kernel_ms[i] receives the mean duration of kernel i.  n_kernels must be >= the kernels per
+ * step (pm_get_param "kernels_per_step"). */
+PM_API pm_status pm_profile_steps(pm_sim* sim, uint32_t nsteps, float* kernel_ms, uint32_t n_kernels);
 
 #ifdef __cplusplus
 }

@@ -48,6 +48,8 @@ SIGNATURES = {
     "pm_get_stats": [_vp, _dp, _dp, _dp, _up],
     "pm_get_grid": [_vp, _dp, _up, _fp, _fp, _fp, _fp, _fp, _fp],
     "pm_set_return_map": [_vp, C.c_int],
+    "pm_get_stream": [_vp, C.POINTER(C.c_void_p)],
+    "pm_profile_steps": [_vp, C.c_uint32, _fp, C.c_uint32],
 }
 
 
@@ -73,6 +75,8 @@ def lib() -> C.CDLL:
         f.restype = C.c_int
     L.pm_last_error_message.restype = C.c_char_p
     L.pm_last_error_message.argtypes = []
+    L.pm_kernel_name.restype = C.c_char_p
+    L.pm_kernel_name.argtypes = [C.c_int]
     _lib = L
     return L
 

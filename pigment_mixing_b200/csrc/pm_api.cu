@@ -457,6 +457,7 @@ pm_status pm_get_param(pm_sim* sim, const char* name, double* out) {
   else if (k == "n_active") *out = c->n_active;
   else if (k == "plastic_count") *out = c->plastic_count;
   else if (k == "grid_nodes") *out = c->n_nodes;
+  else if (k == "kernels_per_step") *out = kernels_per_step();
   else if (k == "Np") *out = sim->np;
   else if (k == "fps") *out = h.fps;
   else if (k == "cfl") *out = h.cfl;
@@ -583,19 +584,21 @@ pm_status pm_set_particles(pm_sim* sim, uint32_t n, const float* x, const float*
   CK(cudaMalloc(&sim->d_sorted, S * sizeof(uint32_t)));
   CK(cudaMalloc(&sim->d_unperm, (size_t)std::max(n, 1u) * F_COUNT * sizeof(float)));
   CK(cudaMalloc(&sim->d_active, std::max(n, 1u)));
-  std::vector<float> h(S * F_COUNT, 0.f);
-  std::vector<uint32_t> meta(S, 0);
-  for (uint32_t p = 0; p < n; ++p) {
-    for (int d = 0; d < 3; ++d) {
-      h[(F_X + d) * S + p] = x[3 * p + d];
-      h[(F_V + d) * S + p] = v ? v[3 * p + d] : 0.f;
-    }
-    h[(F_F + 0) * S + p] = 1.f; h[(F_F + 4) * S + p] = 1.f; h[(F_F + 8) * S + p] = 1.f;
-    if (latent) for (int k = 0; k < 7; ++k) h[(F_LAT + k) * S + p] = latent[7 * p + k];
-    meta[p] = p;
+  // stage the host arrays on the device (d_unperm holds n*42 floats >= n*13) and scatter them
+  // into the structure-of-arrays state there
+  float* dx_ = sim->d_unperm;
+  float* dl_ = dx_ + (size_t)n * 3;
+  float* dv_ = dl_ + (size_t)n * 7;
+  if (n > 0) {
+    CK(cudaMemcpyAsync(dx_, x, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
+    if (latent) CK(cudaMemcpyAsync(dl_, latent, (size_t)n * 7 * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
+    if (v) CK(cudaMemcpyAsync(dv_, v, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
   }
-  CK(cudaMemcpyAsync(sim->d_pbuf[0], h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
-  CK(cudaMemcpyAsync(sim->d_meta[0], meta.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice, sim->stream));
+  Params up{};
+  up.np = (int)n;
+  up.np_stride = (int)S;
+  launch_upload(up, dx_, latent ? dl_ : nullptr, v ? dv_ : nullptr, sim->d_pbuf[0], sim->d_meta[0], sim->stream);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(sim->stream));
   sim->cur = 0;
   sim->prepared = false;
@@ -616,15 +619,10 @@ pm_status pm_get_particles(pm_sim* sim, float* x, float* v, float* latent, float
   p.np_stride = sim->np_stride;
   launch_unpermute(p, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], sim->d_unperm, sim->d_active, sim->stream);
   CK(cudaGetLastError());
-  std::vector<float> tmp;
   auto fetch = [&](int f0, int nf, float* dst) -> pm_status {
     if (!dst) return PM_OK;
-    tmp.resize((size_t)n * nf);
-    CK(cudaMemcpyAsync(tmp.data(), sim->d_unperm + (size_t)f0 * n, (size_t)n * nf * sizeof(float), cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(dst, sim->d_unperm + (size_t)f0 * n, (size_t)n * nf * sizeof(float), cudaMemcpyDeviceToHost,
                        sim->stream));
-    CK(cudaStreamSynchronize(sim->stream));
-    for (uint32_t q = 0; q < n; ++q)
-      for (int k = 0; k < nf; ++k) dst[(size_t)q * nf + k] = tmp[(size_t)k * n + q];
     return PM_OK;
   };
   pm_status s;
@@ -635,10 +633,8 @@ pm_status pm_get_particles(pm_sim* sim, float* x, float* v, float* latent, float
   if ((s = fetch(F_F, 9, F)) != PM_OK) return s;
   if ((s = fetch(F_B, 9, Bm)) != PM_OK) return s;
   if ((s = fetch(F_EPD, 4, plastic)) != PM_OK) return s;
-  if (active) {
-    CK(cudaMemcpyAsync(active, sim->d_active, n, cudaMemcpyDeviceToHost, sim->stream));
-    CK(cudaStreamSynchronize(sim->stream));
-  }
+  if (active) CK(cudaMemcpyAsync(active, sim->d_active, n, cudaMemcpyDeviceToHost, sim->stream));
+  CK(cudaStreamSynchronize(sim->stream));
   return PM_OK;
 }
 
@@ -1036,6 +1032,45 @@ pm_status pm_set_return_map(pm_sim* sim, int mode) {
   sim->return_map = mode;
   if (sim->prepared) sim->fill_params();
   return PM_OK;
+}
+
+pm_status pm_get_stream(pm_sim* sim, void** stream) {
+  if (!sim || !stream) return fail(PM_ERR_INVALID, "NULL argument");
+  *stream = (void*)sim->stream;
+  return PM_OK;
+}
+
+const char* pm_kernel_name(int index) { return kernel_name(index); }
+
+pm_status pm_profile_steps(pm_sim* sim, uint32_t nsteps, float* kernel_ms, uint32_t n_kernels) {
+  if (!sim || !kernel_ms) return fail(PM_ERR_INVALID, "NULL argument");
+  if (!sim->prepared) return fail(PM_ERR_STATE, "call pm_prepare first");
+  const int K = kernels_per_step();
+  if ((int)n_kernels < K) return fail(PM_ERR_INVALID, "kernel_ms needs kernels_per_step entries");
+  CK(cudaSetDevice(sim->device));
+  std::vector<cudaEvent_t> ev(13);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  std::vector<double> acc(K, 0.0);
+  uint32_t done_steps = 0;
+  pm_status st = PM_OK;
+  for (uint32_t k = 0; k < nsteps && st == PM_OK; ++k) {
+    launch_step_timed(sim->P, sim->bufs(sim->cur), sim->stream, ev.data());
+    if (cudaStreamSynchronize(sim->stream) != cudaSuccess) { st = fail(PM_ERR_CUDA, "profiled step failed"); break; }
+    for (int i = 0; i < K; ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+      acc[i] += ms;
+    }
+    st = sim->sync_ctrl();
+    if (st != PM_OK) break;
+    if (sim->h_ctrl->halt) { st = fail(PM_ERR_CAPACITY, "grid capacity reached while profiling"); break; }
+    sim->host_step = sim->h_ctrl->step;
+    sim->cur ^= 1;
+    ++done_steps;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int i = 0; i < K; ++i) kernel_ms[i] = done_steps ? (float)(acc[i] / done_steps) : 0.f;
+  return st;
 }
 
 }  // extern "C"

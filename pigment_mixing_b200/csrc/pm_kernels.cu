@@ -1115,13 +1115,14 @@ __device__ void return_map(const Params& P, double dt, const double sg[3], float
           if (it == 59) err |= E_NEWTON_NOCONV;
           double tm = P.perzyna_visc * dg + dt;
           double tmp = dt / tm;
-          double tmp1 = pow(tmp, P.perzyna_exp);
+          // tmp^m and tmp^(m-1) = tmp^m / tmp from one log and one exp
+          double tmp1 = exp(P.perzyna_exp * log(tmp));
+          double tmpm1 = tmp1 / tmp;
           q_yield = P.q_min + (P.q_max - P.q_min) * exp(-P.xi * ((double)epd + dg / dpre));
           double res = (q_trial - fmu * dg) * tmp1 - q_yield;
           if (fabs(res) < 1e-2) break;
           double qyd = -P.xi / dpre * (P.q_max - P.q_min) * exp(-P.xi * ((double)epd + dg / dpre));
-          double rd = -fmu * tmp1 + (q_trial - fmu * dg) * P.perzyna_exp * pow(tmp, P.perzyna_exp - 1.0) *
-                                        (-P.perzyna_visc * dt) / (tm * tm) - qyd;
+          double rd = -fmu * tmp1 + (q_trial - fmu * dg) * P.perzyna_exp * tmpm1 * (-P.perzyna_visc * dt) / (tm * tm) - qyd;
           if (fabs(rd) < 1e-14) err |= E_NEWTON_FLAT;
           dg -= res / rd;
           if (dg < 0) dg = 1e-10;
@@ -1165,11 +1166,11 @@ __device__ void return_map(const Params& P, double dt, const double sg[3], float
           if (it == 59) err |= E_NEWTON_NOCONV;
           double tm = P.perzyna_visc * dg + dt;
           double tmp = dt / tm;
-          double tmp1 = pow(tmp, P.perzyna_exp);
+          double tmp1 = exp(P.perzyna_exp * log(tmp));
+          double tmpm1 = tmp1 / tmp;
           double res = (q_trial - fmu * dg) * tmp1 - q_yield;
           if (fabs(res) < 1e-2) break;
-          double rd = -fmu * tmp1 + (q_trial - fmu * dg) * P.perzyna_exp * pow(tmp, P.perzyna_exp - 1.0) *
-                                        (-P.perzyna_visc * dt) / (tm * tm);
+          double rd = -fmu * tmp1 + (q_trial - fmu * dg) * P.perzyna_exp * tmpm1 * (-P.perzyna_visc * dt) / (tm * tm);
           if (fabs(rd) < 1e-14) err |= E_NEWTON_FLAT;
           dg -= res / rd;
           if (dg < 0) dg = 1e-10;
@@ -1413,15 +1414,45 @@ __global__ void __launch_bounds__(kThreads) k_reduce_state(Params P, const float
   }
 }
 
-// Copy particle fields back to the original order: out[f][pid] = cur[f][i].
+// Copy particle fields back to the original order, grouped as host arrays: field group g
+// (x, v, B, F, latent, diffusion, plastic, tau) of particle pid lands at
+// out[g_base * np + pid * g_width + component].
+__constant__ int c_group_base[F_COUNT] = {0, 0, 0, 3, 3, 3, 6, 6, 6, 6, 6, 6, 6, 6, 6, 15, 15, 15, 15, 15, 15, 15, 15, 15,
+                                          24, 24, 24, 24, 24, 24, 24, 31, 32, 32, 32, 32, 36, 36, 36, 36, 36, 36};
+__constant__ int c_group_width[F_COUNT] = {3, 3, 3, 3, 3, 3, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9,
+                                           7, 7, 7, 7, 7, 7, 7, 1, 4, 4, 4, 4, 6, 6, 6, 6, 6, 6};
 __global__ void k_unpermute(Params P, const float* pcur, const uint32_t* meta, float* out, uint8_t* active_out) {
   const int S = P.np_stride, np = P.np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
     const uint32_t m = meta[i];
     const uint32_t pid = m & ~kInactiveBit;
     if (pid >= (uint32_t)np) continue;
-    for (int f = 0; f < F_COUNT; ++f) out[(size_t)f * np + pid] = pcur[f * S + i];
+    for (int f = 0; f < F_COUNT; ++f) {
+      const int gb = c_group_base[f], gw = c_group_width[f];
+      out[(size_t)gb * np + (size_t)pid * gw + (f - gb)] = pcur[f * S + i];
+    }
     active_out[pid] = (m & kInactiveBit) ? 0 : 1;
+  }
+}
+
+// Host arrays (x[n*3], latent[n*7], v[n*3] or null) staged on the device -> SoA state with
+// F = I, B = 0 and zero plastic state, meta = particle id.
+__global__ void k_upload(Params P, const float* x, const float* lat, const float* v, float* pbuf, uint32_t* meta) {
+  const int S = P.np_stride, np = P.np;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < S; p += gridDim.x * blockDim.x) {
+    const bool in = p < np;
+    for (int f = 0; f < F_COUNT; ++f) pbuf[f * S + p] = 0.f;
+    if (in) {
+      for (int d = 0; d < 3; ++d) {
+        pbuf[(F_X + d) * S + p] = x[3 * p + d];
+        pbuf[(F_V + d) * S + p] = v ? v[3 * p + d] : 0.f;
+      }
+      if (lat) for (int k = 0; k < 7; ++k) pbuf[(F_LAT + k) * S + p] = lat[7 * p + k];
+      pbuf[(F_F + 0) * S + p] = 1.f;
+      pbuf[(F_F + 4) * S + p] = 1.f;
+      pbuf[(F_F + 8) * S + p] = 1.f;
+    }
+    meta[p] = in ? (uint32_t)p : kInactiveBit;
   }
 }
 
@@ -1485,6 +1516,36 @@ void launch_step(const Params& P, const Bufs& B, cudaStream_t s) {
 }
 
 int kernels_per_step() { return 12; }
+
+static const char* kKernelNames[12] = {"k_prologue", "k_clear", "k_count", "k_scan_local", "k_scan_top", "k_scan_add",
+                                       "k_scatter", "k_p2g", "k_grid_update", "k_g2p_musl", "k_defgrad", "k_epilogue"};
+const char* kernel_name(int i) { return (i >= 0 && i < 12) ? kKernelNames[i] : ""; }
+
+// The same 12 launches with an event recorded after each (events[0] before the first).
+void launch_step_timed(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev) {
+  const int sms = g_num_sms > 0 ? g_num_sms : 148;
+  const int flat_grid = sms * 8;
+  const int scan_blocks = (P.node_cap + 1 + kScanBlock - 1) / kScanBlock;
+  cudaEventRecord(ev[0], s);
+  k_prologue<<<1, 32, 0, s>>>(P, B); cudaEventRecord(ev[1], s);
+  k_clear<<<flat_grid, 256, 0, s>>>(P, B); cudaEventRecord(ev[2], s);
+  k_count<<<flat_grid, 256, 0, s>>>(P, B); cudaEventRecord(ev[3], s);
+  k_scan_local<<<scan_blocks, kScanThreads, 0, s>>>(P, B); cudaEventRecord(ev[4], s);
+  k_scan_top<<<1, kScanThreads, 0, s>>>(P, B); cudaEventRecord(ev[5], s);
+  k_scan_add<<<scan_blocks, kScanThreads, 0, s>>>(P, B); cudaEventRecord(ev[6], s);
+  k_scatter<<<flat_grid, 256, 0, s>>>(P, B); cudaEventRecord(ev[7], s);
+  k_p2g<<<sms * g_occ_p2g, kThreads, p2g_smem_bytes(), s>>>(P, B); cudaEventRecord(ev[8], s);
+  k_grid_update<<<flat_grid, 256, 0, s>>>(P, B); cudaEventRecord(ev[9], s);
+  k_g2p_musl<<<sms * g_occ_g2p, kThreads, g2p_smem_bytes(), s>>>(P, B); cudaEventRecord(ev[10], s);
+  k_defgrad<<<sms * g_occ_def, kThreads, 0, s>>>(P, B); cudaEventRecord(ev[11], s);
+  k_epilogue<<<1, 32, 0, s>>>(P, B); cudaEventRecord(ev[12], s);
+}
+
+void launch_upload(const Params& P, const float* x, const float* lat, const float* v, float* pbuf, uint32_t* meta,
+                   cudaStream_t s) {
+  const int sms = g_num_sms > 0 ? g_num_sms : 148;
+  k_upload<<<sms * 4, 256, 0, s>>>(P, x, lat, v, pbuf, meta);
+}
 
 void launch_reduce_state(const Params& P, const float* pcur, const uint32_t* meta, Ctrl* ctrl, cudaStream_t s) {
   const int sms = g_num_sms > 0 ? g_num_sms : 148;

@@ -17,6 +17,10 @@ void launch_step(const Params& P, const Bufs& B, cudaStream_t s);
 void launch_reduce_state(const Params& P, const float* pcur, const uint32_t* meta, Ctrl* ctrl, cudaStream_t s);
 void launch_unpermute(const Params& P, const float* pcur, const uint32_t* meta, float* out, uint8_t* active,
                       cudaStream_t s);
+const char* kernel_name(int i);
+void launch_step_timed(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev /* 13 events */);
+void launch_upload(const Params& P, const float* x, const float* lat, const float* v, float* pbuf, uint32_t* meta,
+                   cudaStream_t s);
 void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, double* acc, cudaStream_t s);
 
 }  // namespace pm

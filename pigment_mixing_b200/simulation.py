@@ -23,7 +23,7 @@ _SCALARS = ("cfl", "cfl_elastic", "flip_ratio", "rho", "E", "nu", "fps", "end_fr
             "perzyna_visc", "xi", "q_prefac", "pigment_D_max", "pigment_D_edge0", "pigment_D_edge1",
             "start_boost_time", "end_boost_time", "boost_factor", "auto_frame")
 _READONLY = ("time", "dt", "step", "Np", "mu", "lambda", "K", "dt_max", "frame_dt", "final_time",
-             "n_active", "plastic_count", "grid_nodes", "frame")
+             "n_active", "plastic_count", "grid_nodes", "frame", "kernels_per_step")
 _VECTORS = ("gravity", "particle_boundary_min", "particle_boundary_max", "grid_reference_point")
 
 
@@ -195,9 +195,27 @@ class Simulation:
             arrs["active"] = act
         return Particles(arrs)
 
+    def readInto(self, x=None, latent=None, diffusion=None, v=None) -> None:
+        """Copy particle fields into caller-owned float32 arrays (e.g. pinned host buffers)."""
+        call("pm_get_particles", self._h, _fp(x), _fp(v), _fp(latent), _fp(diffusion), None, None, None, None)
+
     @property
     def particles(self) -> Particles:
         return self.getParticles()
+
+    def stream(self) -> int:
+        """cudaStream_t (as an integer) on which all of this simulation's kernels run."""
+        p = C.c_void_p()
+        call("pm_get_stream", self._h, C.byref(p))
+        return p.value or 0
+
+    def profileSteps(self, nsteps: int) -> dict:
+        """Mean CUDA-event duration (ms) of every kernel of a step over nsteps steps."""
+        from ._lib import lib
+        k = int(self.kernels_per_step)
+        ms = np.zeros(k, np.float32)
+        call("pm_profile_steps", self._h, int(nsteps), _fp(ms), k)
+        return {lib().pm_kernel_name(i).decode(): float(ms[i]) for i in range(k)}
 
     def errorFlags(self, clear: bool = False) -> int:
         f = C.c_uint32()
