@@ -173,6 +173,27 @@ PM_API const char* pm_kernel_name(int index);
  * step (pm_get_param "kernels_per_step"). */
 PM_API pm_status pm_profile_steps(pm_sim* sim, uint32_t nsteps, float* kernel_ms, uint32_t n_kernels);
 
+/* ---- particle-to-grid transfer that allocates nothing --------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc: code running while
+ * a CUDA graph is captured, and plug-ins whose host application owns every device allocation.
+ * It scatters caller-owned particle arrays onto a caller-described node box with the step's
+ * P2G transfer (quadratic B-splines, counting sort by cell, one warp per cell) and the
+ * reference's normalisation (p2g.cpp:97-124).  Inputs and outputs are device pointers:
+ * x[n*3], v[n*3], B[n*9] (APIC matrix, NULL = none), latent[n*7], diffusion[n]; node (i,j,k) sits
+ * at origin + (i,j,k)*dx and is entry (i*dims[1] + j)*dims[2] + k of node_mass[nodes],
+ * node_velocity[nodes*3], node_latent[nodes*7], node_shear[nodes] (any output may be NULL).
+ * Scratch is one fixed 8 MiB __device__ array inside the library (held by every GPU that loads
+ * it until exit): at most 131072 particles and 131072 nodes per call, PM_ERR_CAPACITY beyond.
+ * The first call on a device looks up that array's device address, so make it before any stream
+ * capture.  All calls share the array: calls whose work overlaps on the GPU race.  Work is queued
+ * on `stream` (NULL = default stream); when `outside` is not NULL the call waits for the stream
+ * and stores the number of particles whose stencil left the box (they are skipped). */
+PM_API pm_status pm_p2g_noalloc(const float* x, const float* v, const float* B, const float* latent,
+                                const float* diffusion, uint32_t n, double particle_mass, double dx,
+                                const double origin[3], const int32_t dims[3], float* node_mass,
+                                float* node_velocity, float* node_latent, float* node_shear, void* stream,
+                                uint32_t* outside);
+
 #ifdef __cplusplus
 }
 #endif

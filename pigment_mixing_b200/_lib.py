@@ -50,6 +50,7 @@ SIGNATURES = {
     "pm_set_return_map": [_vp, C.c_int],
     "pm_get_stream": [_vp, C.POINTER(C.c_void_p)],
     "pm_profile_steps": [_vp, C.c_uint32, _fp, C.c_uint32],
+    "pm_p2g_noalloc": [_vp] * 5 + [C.c_uint32, C.c_double, C.c_double, _dp, C.POINTER(C.c_int32)] + [_vp] * 5 + [_up],
 }
 
 
