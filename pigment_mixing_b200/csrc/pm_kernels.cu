@@ -430,19 +430,23 @@ __global__ void k_scatter(Params P, Bufs B) {
 // ------------------------------------------------------------------------------------------
 // P2G: warp per cell, lane per stencil node, shared 6x6x6 tile per brick
 // ------------------------------------------------------------------------------------------
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;  // threads per CTA of the brick kernels
 constexpr int kWarps = kThreads / 32;
 constexpr int kP2GCh = 15;
 
+// Per-particle data staged by a warp for its node-parallel scatter: the values every lane reads
+// are grouped into float4s (one 128-bit broadcast load each), the per-axis weights follow.
 struct __align__(16) StageP2G {
-  float N[9];     // Nx[3], Ny[3], Nz[3]
-  float dN[9];    // dNx, dNy, dNz (times inv_dx)
-  float q[3];     // v - D * B r
-  float Cc[9];    // D * dx * B columns: C0 xyz, C1 xyz, C2 xyz
-  float tau[6];   // xx yy zz xy xz yz
-  float lat[7];
-  float diff;
-  float pad[4];
+  float4 a;   // q0 q1 q2 diff           (q = v - D B r)
+  float4 c0;  // C0x C0y C0z C1x         (C = D dx B, columns)
+  float4 c1;  // C1y C1z C2x C2y
+  float4 c2;  // C2z tau_xx tau_yy tau_zz
+  float4 t;   // tau_xy tau_xz tau_yz lat0
+  float4 l0;  // lat1 lat2 lat3 lat4
+  float4 l1;  // lat5 lat6 - -
+  float N[9];   // Nx[3], Ny[3], Nz[3]
+  float dN[9];  // derivatives times inv_dx
+  float pad[2];
 };
 static_assert(sizeof(StageP2G) == 48 * 4, "stage size");
 
@@ -463,96 +467,124 @@ __device__ __forceinline__ int tile_to_node(int tn, int bx, int by, int bz, cons
   return ((gx * c->nb[1] + gy) * c->nb[2] + gz) * kBrickNodes + (tx & 3) * 16 + (ty & 3) * 4 + (tz & 3);
 }
 
+// Local cell (0..63, lx*16 + ly*4 + lz) of a particle inside brick (bx, by, bz), clamped.
+__device__ __forceinline__ int local_cell(const AxisW aw[3], const Ctrl* c, int bx, int by, int bz) {
+  const int lx = min(max(aw[0].base - c->g0[0] - bx * 4, 0), 3);
+  const int ly = min(max(aw[1].base - c->g0[1] - by * 4, 0), 3);
+  const int lz = min(max(aw[2].base - c->g0[2] - bz * 4, 0), 3);
+  return lx * 16 + ly * 4 + lz;
+}
+
+// One CTA per brick (grid-stride).  Each warp takes 32 consecutive particles of the brick's
+// sorted range: lane i stages particle i (weights, APIC terms, stress, latent), then the warp
+// walks the runs of equal cells in its 32 particles (found with a ballot) and, for each run,
+// lane l < 27 accumulates the run's particles into stencil node l in registers and adds the
+// sums once to the brick's shared 6x6x6 tile.  Block barriers only around the tile.
 __global__ void __launch_bounds__(kThreads) k_p2g(Params P, Bufs B) {
   const Ctrl* c = B.ctrl;
   if (c->halt) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* tile = reinterpret_cast<float*>(smem_raw);                       // [kP2GCh][216]
-  StageP2G* st = reinterpret_cast<StageP2G*>(tile + kP2GCh * kTileNodes);  // [kThreads]
+  StageP2G* stw = reinterpret_cast<StageP2G*>(tile + kP2GCh * kTileNodes);  // [kWarps][32]
   const int S = P.np_stride;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  StageP2G* st = stw + warp * 32;
   const int la = lane / 9, lb = (lane / 3) % 3, lc = lane % 3;
+  const float fa = (float)la, fb = (float)lb, fc = (float)lc;
   const float D = P.apicD, dx = P.dx;
   const bool apic = P.flip_ratio < 0.f;
   const int nbr = c->n_bricks;
   for (int b = blockIdx.x; b < nbr; b += gridDim.x) {
-    const uint32_t* cs = B.cell + (size_t)b * kBrickNodes;
-    const uint32_t ps = cs[0], pe = cs[kBrickNodes];
+    const uint32_t ps = B.cell[(size_t)b * kBrickNodes], pe = B.cell[(size_t)(b + 1) * kBrickNodes];
     if (ps == pe) continue;
     int bx, by, bz;
     brick_coords(b, c, bx, by, bz);
     for (int i = threadIdx.x; i < kP2GCh * kTileNodes; i += kThreads) tile[i] = 0.f;
-    for (uint32_t c0 = ps; c0 < pe; c0 += kThreads) {
-      const uint32_t c1 = min(c0 + (uint32_t)kThreads, pe);
-      __syncthreads();  // tile zeroed / previous chunk consumed
-      if (c0 + threadIdx.x < c1) {
-        const uint32_t o = B.sorted[c0 + threadIdx.x];
-        StageP2G& s = st[threadIdx.x];
-        float xp[3], r[3];
+    __syncthreads();
+    for (uint32_t c0 = ps + 32u * warp; c0 < pe; c0 += 32u * kWarps) {
+      const int n = (int)min(32u, pe - c0);
+      int cl = -1;
+      if (lane < n) {
+        const uint32_t o = B.sorted[c0 + lane];
+        StageP2G& sp = st[lane];
+        AxisW aw[3];
+        float r[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          xp[d] = B.pin[(F_X + d) * S + o];
-          AxisW aw = axis_weights(xp[d], P.anchor[d], dx, P.inv_dx);
-          r[d] = aw.r;
+          aw[d] = axis_weights(B.pin[(F_X + d) * S + o], P.anchor[d], dx, P.inv_dx);
+          r[d] = aw[d].r;
 #pragma unroll
-          for (int k = 0; k < 3; ++k) { s.N[3 * d + k] = aw.N[k]; s.dN[3 * d + k] = aw.dN[k]; }
+          for (int k = 0; k < 3; ++k) { sp.N[3 * d + k] = aw[d].N[k]; sp.dN[3 * d + k] = aw[d].dN[k]; }
         }
-        float v[3], Bm[9];
+        cl = local_cell(aw, c, bx, by, bz);
+        float v[3], Bm[9], q[3], C[9];
 #pragma unroll
         for (int d = 0; d < 3; ++d) v[d] = B.pin[(F_V + d) * S + o];
 #pragma unroll
         for (int k = 0; k < 9; ++k) Bm[k] = apic ? B.pin[(F_B + k) * S + o] : 0.f;
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          float Br = Bm[3 * i] * r[0] + Bm[3 * i + 1] * r[1] + Bm[3 * i + 2] * r[2];
-          s.q[i] = v[i] - D * Br;
-        }
+        for (int i = 0; i < 3; ++i) q[i] = v[i] - D * (Bm[3 * i] * r[0] + Bm[3 * i + 1] * r[1] + Bm[3 * i + 2] * r[2]);
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
-          for (int i = 0; i < 3; ++i) s.Cc[3 * k + i] = D * dx * Bm[3 * i + k];
+          for (int i = 0; i < 3; ++i) C[3 * k + i] = D * dx * Bm[3 * i + k];
+        float tau[6], lat[7];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) s.tau[k] = B.pin[(F_TAU + k) * S + o];
+        for (int k = 0; k < 6; ++k) tau[k] = B.pin[(F_TAU + k) * S + o];
 #pragma unroll
-        for (int k = 0; k < 7; ++k) s.lat[k] = B.pin[(F_LAT + k) * S + o];
-        s.diff = B.pin[F_DIFF * S + o];
+        for (int k = 0; k < 7; ++k) lat[k] = B.pin[(F_LAT + k) * S + o];
+        sp.a = make_float4(q[0], q[1], q[2], B.pin[F_DIFF * S + o]);
+        sp.c0 = make_float4(C[0], C[1], C[2], C[3]);
+        sp.c1 = make_float4(C[4], C[5], C[6], C[7]);
+        sp.c2 = make_float4(C[8], tau[0], tau[1], tau[2]);
+        sp.t = make_float4(tau[3], tau[4], tau[5], lat[0]);
+        sp.l0 = make_float4(lat[1], lat[2], lat[3], lat[4]);
+        sp.l1 = make_float4(lat[5], lat[6], 0.f, 0.f);
       }
-      __syncthreads();
-      for (int cl = warp; cl < kBrickNodes; cl += kWarps) {
-        const uint32_t s0 = max(cs[cl], c0), s1 = min(cs[cl + 1], c1);
-        if (s0 >= s1) continue;
+      // runs of equal cells among the warp's particles
+      const int prev = __shfl_up_sync(0xffffffffu, cl, 1);
+      uint32_t heads = __ballot_sync(0xffffffffu, lane < n && (lane == 0 || cl != prev));
+      __syncwarp();
+      while (heads) {
+        const int s0 = __ffs(heads) - 1;
+        heads &= heads - 1;
+        const int s1 = heads ? __ffs(heads) - 1 : n;
+        const int cell = __shfl_sync(0xffffffffu, cl, s0);
         if (lane < 27) {
           float acc[kP2GCh];
 #pragma unroll
           for (int k = 0; k < kP2GCh; ++k) acc[k] = 0.f;
-          const float fa = (float)la, fb = (float)lb, fc = (float)lc;
-          for (uint32_t sp = s0; sp < s1; ++sp) {
-            const StageP2G& s = st[sp - c0];
-            const float nx = s.N[la], ny = s.N[3 + lb], nz = s.N[6 + lc];
+          for (int q = s0; q < s1; ++q) {
+            const StageP2G& sp = st[q];
+            const float nx = sp.N[la], ny = sp.N[3 + lb], nz = sp.N[6 + lc];
             const float nyz = ny * nz;
             const float w = nx * nyz;
-            const float gx = s.dN[la] * nyz, gy = nx * s.dN[3 + lb] * nz, gz = nx * ny * s.dN[6 + lc];
+            const float gx = sp.dN[la] * nyz, gy = nx * sp.dN[3 + lb] * nz, gz = nx * ny * sp.dN[6 + lc];
             const float wm = w > 1e-25f ? w : 0.f;  // p2g.cpp:39
+            const float4 A = sp.a, C0 = sp.c0, C1 = sp.c1, C2 = sp.c2, T = sp.t, L0 = sp.l0, L1 = sp.l1;
             acc[0] += wm;
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-              float t = s.q[i] + fa * s.Cc[i] + fb * s.Cc[3 + i] + fc * s.Cc[6 + i];
-              acc[1 + i] += wm * t;
-            }
-            acc[4] += s.tau[0] * gx + s.tau[3] * gy + s.tau[4] * gz;
-            acc[5] += s.tau[3] * gx + s.tau[1] * gy + s.tau[5] * gz;
-            acc[6] += s.tau[4] * gx + s.tau[5] * gy + s.tau[2] * gz;
-#pragma unroll
-            for (int k = 0; k < 7; ++k) acc[7 + k] += wm * s.lat[k];
-            acc[14] += wm * s.diff;
+            acc[1] += wm * (A.x + fa * C0.x + fb * C0.w + fc * C1.z);
+            acc[2] += wm * (A.y + fa * C0.y + fb * C1.x + fc * C1.w);
+            acc[3] += wm * (A.z + fa * C0.z + fb * C1.y + fc * C2.x);
+            acc[4] += C2.y * gx + T.x * gy + T.y * gz;
+            acc[5] += T.x * gx + C2.z * gy + T.z * gz;
+            acc[6] += T.y * gx + T.z * gy + C2.w * gz;
+            acc[7] += wm * T.w;
+            acc[8] += wm * L0.x;
+            acc[9] += wm * L0.y;
+            acc[10] += wm * L0.z;
+            acc[11] += wm * L0.w;
+            acc[12] += wm * L1.x;
+            acc[13] += wm * L1.y;
+            acc[14] += wm * A.w;
           }
-          const int lx = cl >> 4, ly = (cl >> 2) & 3, lz = cl & 3;
-          const int tn = ((lx + la) * kTile + (ly + lb)) * kTile + (lz + lc);
+          const int tn = (((cell >> 4) + la) * kTile + (((cell >> 2) & 3) + lb)) * kTile + ((cell & 3) + lc);
 #pragma unroll
           for (int k = 0; k < kP2GCh; ++k)
             if (acc[k] != 0.f) atomicAdd(&tile[k * kTileNodes + tn], acc[k]);
         }
       }
+      __syncwarp();
     }
     __syncthreads();
     for (int tn = threadIdx.x; tn < kTileNodes; tn += kThreads) {
@@ -790,10 +822,11 @@ __global__ void k_grid_update(Params P, Bufs B) {
     const int gi[3] = {c->g0[0] + bx * 4 + (loc >> 4), c->g0[1] + by * 4 + ((loc >> 2) & 3), c->g0[2] + bz * 4 + (loc & 3)};
     float X[3] = {node_pos(gi[0], P.anchor[0], P.dx), node_pos(gi[1], P.anchor[1], P.dx), node_pos(gi[2], P.anchor[2], P.dx)};
     boundary_collision(c, dtf, P.dx, X, nv, err);
-    rec[0] = make_float4(mi, nv[0], nv[1], nv[2]);
-    rec[1] = make_float4(nv[0] - v[0], nv[1] - v[1], nv[2] - v[2], lat[0]);
-    rec[2] = make_float4(lat[1], lat[2], lat[3], lat[4]);
-    rec[3] = make_float4(lat[5], lat[6], shear, 0.f);
+    // updated record, laid out as the G2P tile reads it (4 x 16 B per node)
+    rec[0] = make_float4(nv[0], nv[1], nv[2], nv[0] - v[0]);
+    rec[1] = make_float4(nv[1] - v[1], nv[2] - v[2], lat[0], lat[1]);
+    rec[2] = make_float4(lat[2], lat[3], lat[4], lat[5]);
+    rec[3] = make_float4(lat[6], shear, mi, 0.f);
   }
   if (err) atomicOr(&B.ctrl->error_flags, err);
 }
@@ -801,17 +834,18 @@ __global__ void k_grid_update(Params P, Bufs B) {
 // ------------------------------------------------------------------------------------------
 // G2P + mixing + MUSL (velocity update and re-scatter)
 // ------------------------------------------------------------------------------------------
-constexpr int kG2PCh = 14;  // v3 flip3 lat7 shear1
 struct __align__(16) StageMUSL {
+  float4 q;    // q0 q1 q2 -   (q = v_new - D B_new r)
+  float4 c0;   // C0x C0y C0z C1x
+  float4 c1;   // C1y C1z C2x C2y
+  float4 c2;   // C2z - - -
   float N[9];
-  float q[3];
-  float Cc[9];
   float pad[3];
 };
-static_assert(sizeof(StageMUSL) == 24 * 4, "stage size");
+static_assert(sizeof(StageMUSL) == 28 * 4, "stage size");
 
 size_t g2p_smem_bytes() {
-  return sizeof(float) * (kG2PCh + 4) * kTileNodes + sizeof(StageMUSL) * kThreads;
+  return sizeof(float4) * 4 * kTileNodes + sizeof(float) * 4 * kTileNodes + sizeof(StageMUSL) * kThreads;
 }
 
 __device__ __forceinline__ float smooth_step(float e0, float e1, float x) {  // g2p.cpp:7-10
@@ -819,16 +853,23 @@ __device__ __forceinline__ float smooth_step(float e0, float e1, float x) {  // 
   return t * t * (3.f - 2.f * t);
 }
 
-__global__ void __launch_bounds__(kThreads) k_g2p_musl(Params P, Bufs B) {
+// One CTA per brick.  The brick's 6x6x6 node tile (updated records, 4 x float4 per node) is
+// loaded once; each warp then takes 32 consecutive particles of the brick's sorted range: lane i
+// gathers G2P for particle i, writes its new state in sorted order and stages its MUSL data; the
+// warp then scatters the staged particles run by run of equal cells, lane l < 27 owning stencil
+// node l, into the brick's shared MUSL tile, flushed once per brick.
+__global__ void __launch_bounds__(kThreads, 5) k_g2p_musl(Params P, Bufs B) {
   const Ctrl* c = B.ctrl;
   if (c->halt) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float* tile = reinterpret_cast<float*>(smem_raw);     // [14][216]
-  float* mtile = tile + kG2PCh * kTileNodes;             // [4][216]
-  StageMUSL* st = reinterpret_cast<StageMUSL*>(mtile + 4 * kTileNodes);
+  float4* tile = reinterpret_cast<float4*>(smem_raw);              // [216][4]
+  float* mtile = reinterpret_cast<float*>(tile + 4 * kTileNodes);  // [4][216]
+  StageMUSL* stw = reinterpret_cast<StageMUSL*>(mtile + 4 * kTileNodes);
   const int S = P.np_stride;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  StageMUSL* st = stw + warp * 32;
   const int la = lane / 9, lb = (lane / 3) % 3, lc = lane % 3;
+  const float fa = (float)la, fb = (float)lb, fcc = (float)lc;
   const float D = P.apicD, dx = P.dx;
   const float fr = P.flip_ratio;
   const bool apic = fr < 0.f, use_flip = fr >= -1.f, musl = P.use_musl != 0;
@@ -846,27 +887,21 @@ __global__ void __launch_bounds__(kThreads) k_g2p_musl(Params P, Bufs B) {
   const float dyn = P.D_max * time_factor;
   const int nbr = c->n_bricks;
   for (int b = blockIdx.x; b < nbr; b += gridDim.x) {
-    const uint32_t* cs = B.cell + (size_t)b * kBrickNodes;
-    const uint32_t ps = cs[0], pe = cs[kBrickNodes];
+    const uint32_t ps = B.cell[(size_t)b * kBrickNodes], pe = B.cell[(size_t)(b + 1) * kBrickNodes];
     if (ps == pe) continue;
     int bx, by, bz;
     brick_coords(b, c, bx, by, bz);
-    __syncthreads();
     for (int i = threadIdx.x; i < kTileNodes * 4; i += kThreads) {
-      const int tn = i >> 2, part = i & 3;
-      const int node = tile_to_node(tn, bx, by, bz, c);
-      float4 r = node >= 0 ? B.grid[(size_t)node * 4 + part] : make_float4(0.f, 0.f, 0.f, 0.f);
-      if (part == 0) { tile[0 * kTileNodes + tn] = r.y; tile[1 * kTileNodes + tn] = r.z; tile[2 * kTileNodes + tn] = r.w; }
-      else if (part == 1) { tile[3 * kTileNodes + tn] = r.x; tile[4 * kTileNodes + tn] = r.y; tile[5 * kTileNodes + tn] = r.z; tile[6 * kTileNodes + tn] = r.w; }
-      else if (part == 2) { tile[7 * kTileNodes + tn] = r.x; tile[8 * kTileNodes + tn] = r.y; tile[9 * kTileNodes + tn] = r.z; tile[10 * kTileNodes + tn] = r.w; }
-      else { tile[11 * kTileNodes + tn] = r.x; tile[12 * kTileNodes + tn] = r.y; tile[13 * kTileNodes + tn] = r.z; }
+      const int node = tile_to_node(i >> 2, bx, by, bz, c);
+      tile[i] = node >= 0 ? B.grid[(size_t)node * 4 + (i & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
     for (int i = threadIdx.x; i < 4 * kTileNodes; i += kThreads) mtile[i] = 0.f;
-    for (uint32_t c0 = ps; c0 < pe; c0 += kThreads) {
-      const uint32_t c1 = min(c0 + (uint32_t)kThreads, pe);
-      __syncthreads();
-      if (c0 + threadIdx.x < c1) {
-        const uint32_t i = c0 + threadIdx.x;
+    __syncthreads();
+    for (uint32_t c0 = ps + 32u * warp; c0 < pe; c0 += 32u * kWarps) {
+      const int n = (int)min(32u, pe - c0);
+      int cl = -1;
+      if (lane < n) {
+        const uint32_t i = c0 + lane;
         const uint32_t o = B.sorted[i];
         float xp[3], vold[3], lat[7];
         AxisW aw[3];
@@ -878,12 +913,8 @@ __global__ void __launch_bounds__(kThreads) k_g2p_musl(Params P, Bufs B) {
         }
 #pragma unroll
         for (int k = 0; k < 7; ++k) lat[k] = B.pin[(F_LAT + k) * S + o];
-        // local cell of the particle within the tile
-        // local cell of the particle in its brick (always 0..3 by construction; clamped so a
-        // particle outside the step's box can never index past the tile)
-        const int lx = min(max(aw[0].base - c->g0[0] - bx * 4, 0), 3);
-        const int ly = min(max(aw[1].base - c->g0[1] - by * 4, 0), 3);
-        const int lz = min(max(aw[2].base - c->g0[2] - bz * 4, 0), 3);
+        cl = local_cell(aw, c, bx, by, bz);
+        const int lx = cl >> 4, ly = (cl >> 2) & 3, lz = cl & 3;
         float vp[3] = {0.f, 0.f, 0.f}, fp[3] = {0.f, 0.f, 0.f}, Bp[9], L[9], gl[7], gs = 0.f;
 #pragma unroll
         for (int k = 0; k < 9; ++k) { Bp[k] = 0.f; L[k] = 0.f; }
@@ -896,34 +927,35 @@ __global__ void __launch_bounds__(kThreads) k_g2p_musl(Params P, Bufs B) {
           for (int bb = 0; bb < 3; ++bb) {
             const float dyb = (float)bb * dx - aw[1].r;
             const float nxy = aw[0].N[a] * aw[1].N[bb];
+            const float dnxy = aw[0].dN[a] * aw[1].N[bb], ndxy = aw[0].N[a] * aw[1].dN[bb];
 #pragma unroll
-            for (int cc = 0; cc < 3; ++cc) {
-              const float dzc = (float)cc * dx - aw[2].r;
-              const int tn = ((lx + a) * kTile + (ly + bb)) * kTile + (lz + cc);
-              const float w = nxy * aw[2].N[cc];
-              const float g[3] = {aw[0].dN[a] * aw[1].N[bb] * aw[2].N[cc], aw[0].N[a] * aw[1].dN[bb] * aw[2].N[cc],
-                                  nxy * aw[2].dN[cc]};
-              const float gv[3] = {tile[tn], tile[kTileNodes + tn], tile[2 * kTileNodes + tn]};
+            for (int cz = 0; cz < 3; ++cz) {
+              const float dzc = (float)cz * dx - aw[2].r;
+              const int tn = ((lx + a) * kTile + (ly + bb)) * kTile + (lz + cz);
+              const float w = nxy * aw[2].N[cz];
+              const float g0 = dnxy * aw[2].N[cz], g1 = ndxy * aw[2].N[cz], g2 = nxy * aw[2].dN[cz];
+              const float4 R0 = tile[4 * tn], R1 = tile[4 * tn + 1], R2 = tile[4 * tn + 2], R3 = tile[4 * tn + 3];
+              const float gv[3] = {R0.x, R0.y, R0.z};
 #pragma unroll
               for (int r = 0; r < 3; ++r) {
-                vp[r] += gv[r] * w;
                 const float wv = gv[r] * w;
+                vp[r] += wv;
                 Bp[3 * r + 0] += wv * dxa;
                 Bp[3 * r + 1] += wv * dyb;
                 Bp[3 * r + 2] += wv * dzc;
-                L[3 * r + 0] += gv[r] * g[0];
-                L[3 * r + 1] += gv[r] * g[1];
-                L[3 * r + 2] += gv[r] * g[2];
-                fp[r] += tile[(3 + r) * kTileNodes + tn] * w;
+                L[3 * r + 0] += gv[r] * g0;
+                L[3 * r + 1] += gv[r] * g1;
+                L[3 * r + 2] += gv[r] * g2;
               }
-#pragma unroll
-              for (int k = 0; k < 7; ++k) gl[k] += tile[(6 + k) * kTileNodes + tn] * w;
-              gs += tile[13 * kTileNodes + tn] * w;
+              if (use_flip) { fp[0] += R0.w * w; fp[1] += R1.x * w; fp[2] += R1.y * w; }
+              gl[0] += R1.z * w; gl[1] += R1.w * w;
+              gl[2] += R2.x * w; gl[3] += R2.y * w; gl[4] += R2.z * w; gl[5] += R2.w * w;
+              gl[6] += R3.x * w;
+              gs += R3.y * w;
             }
           }
         }
         if (!apic) for (int k = 0; k < 9; ++k) Bp[k] = 0.f;
-        if (!use_flip) { fp[0] = fp[1] = fp[2] = 0.f; }
         // diffusion factor |0.5 (L + L^T)|_F (g2p.cpp:98-101)
         float s2 = 0.f;
 #pragma unroll
@@ -959,44 +991,54 @@ __global__ void __launch_bounds__(kThreads) k_g2p_musl(Params P, Bufs B) {
         for (int k = 0; k < 7; ++k) po[(F_LAT + k) * S + i] = lat[k];
         po[F_DIFF * S + i] = diff;
         if (musl) {
-          StageMUSL& s = st[threadIdx.x];
+          StageMUSL& sp = st[lane];
 #pragma unroll
           for (int d = 0; d < 3; ++d)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) s.N[3 * d + k] = aw[d].N[k];
+            for (int k = 0; k < 3; ++k) sp.N[3 * d + k] = aw[d].N[k];
           const float r3[3] = {aw[0].r, aw[1].r, aw[2].r};
+          float q[3], C[9];
 #pragma unroll
-          for (int q = 0; q < 3; ++q) {
-            float Br = Bp[3 * q] * r3[0] + Bp[3 * q + 1] * r3[1] + Bp[3 * q + 2] * r3[2];
-            s.q[q] = vnew[q] - D * Br;
-          }
+          for (int qq = 0; qq < 3; ++qq)
+            q[qq] = vnew[qq] - D * (Bp[3 * qq] * r3[0] + Bp[3 * qq + 1] * r3[1] + Bp[3 * qq + 2] * r3[2]);
 #pragma unroll
           for (int k = 0; k < 3; ++k)
 #pragma unroll
-            for (int q = 0; q < 3; ++q) s.Cc[3 * k + q] = D * dx * Bp[3 * q + k];
+            for (int qq = 0; qq < 3; ++qq) C[3 * k + qq] = D * dx * Bp[3 * qq + k];
+          sp.q = make_float4(q[0], q[1], q[2], 0.f);
+          sp.c0 = make_float4(C[0], C[1], C[2], C[3]);
+          sp.c1 = make_float4(C[4], C[5], C[6], C[7]);
+          sp.c2 = make_float4(C[8], 0.f, 0.f, 0.f);
         }
       }
-      __syncthreads();
       if (musl) {
-        for (int cl = warp; cl < kBrickNodes; cl += kWarps) {
-          const uint32_t s0 = max(cs[cl], c0), s1 = min(cs[cl + 1], c1);
-          if (s0 >= s1 || lane >= 27) continue;
-          float acc[4] = {0.f, 0.f, 0.f, 0.f};
-          const float fa = (float)la, fb = (float)lb, fc = (float)lc;
-          for (uint32_t sp = s0; sp < s1; ++sp) {
-            const StageMUSL& s = st[sp - c0];
-            const float w = s.N[la] * s.N[3 + lb] * s.N[6 + lc];
-            const float wm = w > 1e-25f ? w : 0.f;  // musl.cpp:188
+        const int prev = __shfl_up_sync(0xffffffffu, cl, 1);
+        uint32_t heads = __ballot_sync(0xffffffffu, lane < n && (lane == 0 || cl != prev));
+        __syncwarp();
+        while (heads) {
+          const int s0 = __ffs(heads) - 1;
+          heads &= heads - 1;
+          const int s1 = heads ? __ffs(heads) - 1 : n;
+          const int cell = __shfl_sync(0xffffffffu, cl, s0);
+          if (lane < 27) {
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int q = s0; q < s1; ++q) {
+              const StageMUSL& sp = st[q];
+              const float w = sp.N[la] * (sp.N[3 + lb] * sp.N[6 + lc]);
+              const float wm = w > 1e-25f ? w : 0.f;  // musl.cpp:188
+              const float4 Q = sp.q, C0 = sp.c0, C1 = sp.c1, C2 = sp.c2;
+              acc[0] += wm * (Q.x + fa * C0.x + fb * C0.w + fcc * C1.z);
+              acc[1] += wm * (Q.y + fa * C0.y + fb * C1.x + fcc * C1.w);
+              acc[2] += wm * (Q.z + fa * C0.z + fb * C1.y + fcc * C2.x);
+              acc[3] += wm;
+            }
+            const int tn = (((cell >> 4) + la) * kTile + (((cell >> 2) & 3) + lb)) * kTile + ((cell & 3) + lc);
 #pragma unroll
-            for (int q = 0; q < 3; ++q) acc[q] += wm * (s.q[q] + fa * s.Cc[q] + fb * s.Cc[3 + q] + fc * s.Cc[6 + q]);
-            acc[3] += wm;
+            for (int k = 0; k < 4; ++k)
+              if (acc[k] != 0.f) atomicAdd(&mtile[k * kTileNodes + tn], acc[k]);
           }
-          const int lx = cl >> 4, ly = (cl >> 2) & 3, lz = cl & 3;
-          const int tn = ((lx + la) * kTile + (ly + lb)) * kTile + (lz + lc);
-#pragma unroll
-          for (int k = 0; k < 4; ++k)
-            if (acc[k] != 0.f) atomicAdd(&mtile[k * kTileNodes + tn], acc[k]);
         }
+        __syncwarp();
       }
     }
     __syncthreads();
@@ -1009,6 +1051,7 @@ __global__ void __launch_bounds__(kThreads) k_g2p_musl(Params P, Bufs B) {
         red_add_v4(B.gmusl + node, mtile[tn], mtile[kTileNodes + tn], mtile[2 * kTileNodes + tn], w);
       }
     }
+    __syncthreads();
   }
 }
 
@@ -1062,6 +1105,114 @@ __device__ void svd3_d(const double A[9], double U[9], double s[3], double V[9])
   }
   if (zero_cols == 1) {
     int a = (zc + 1) % 3, b = (zc + 2) % 3;
+    U[0 + zc] = U[3 + a] * U[6 + b] - U[6 + a] * U[3 + b];
+    U[3 + zc] = U[6 + a] * U[0 + b] - U[0 + a] * U[6 + b];
+    U[6 + zc] = U[0 + a] * U[3 + b] - U[3 + a] * U[0 + b];
+  } else if (zero_cols > 1) {
+    for (int k = 0; k < 9; ++k) U[k] = (k % 4 == 0) ? 1.0 : 0.0;
+  }
+}
+
+// FP32 cyclic Jacobi rotation of a symmetric 3x3 on pair (p, q); arp, arq are the entries of the
+// third row against p and q; V accumulates the rotations.
+__device__ __forceinline__ void jrot_f32(float& app, float& aqq, float& apq, float& arp, float& arq, float* V, int p,
+                                         int q) {
+  if (fabsf(apq) <= 1e-30f || fabsf(apq) <= 1e-9f * (fabsf(app) + fabsf(aqq))) return;
+  const float zeta = (aqq - app) / (2.f * apq);
+  const float t = copysignf(1.f, zeta) / (fabsf(zeta) + sqrtf(1.f + zeta * zeta));
+  const float cs = rsqrtf(1.f + t * t);
+  const float sn = t * cs;
+  app -= t * apq;
+  aqq += t * apq;
+  apq = 0.f;
+  const float rp = arp, rq = arq;
+  arp = cs * rp - sn * rq;
+  arq = sn * rp + cs * rq;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float vp = V[3 * k + p], vq = V[3 * k + q];
+    V[3 * k + p] = cs * vp - sn * vq;
+    V[3 * k + q] = sn * vp + cs * vq;
+  }
+}
+
+// SVD of a 3x3 with an FP32 warm start: cyclic Jacobi in FP32 on the trace-shifted A^T A gives
+// approximate right singular vectors; they are re-orthonormalised in FP64 and one-sided Jacobi
+// sweeps in FP64 run on W = A V until no column pair needs a rotation, so the result has FP64
+// accuracy (sigma >= 0, U and V orthogonal) with fewer FP64 rotations than a cold start.
+__device__ void svd3_warm(const double A[9], double U[9], double s[3], double V[9]) {
+  double S[6];
+  S[0] = A[0] * A[0] + A[3] * A[3] + A[6] * A[6];
+  S[1] = A[1] * A[1] + A[4] * A[4] + A[7] * A[7];
+  S[2] = A[2] * A[2] + A[5] * A[5] + A[8] * A[8];
+  S[3] = A[0] * A[1] + A[3] * A[4] + A[6] * A[7];
+  S[4] = A[0] * A[2] + A[3] * A[5] + A[6] * A[8];
+  S[5] = A[1] * A[2] + A[4] * A[5] + A[7] * A[8];
+  const double m = (S[0] + S[1] + S[2]) / 3.0;
+  float a00 = (float)(S[0] - m), a11 = (float)(S[1] - m), a22 = (float)(S[2] - m);
+  float a01 = (float)S[3], a02 = (float)S[4], a12 = (float)S[5];
+  float Vf[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
+#pragma unroll 1
+  for (int sweep = 0; sweep < 5; ++sweep) {
+    jrot_f32(a00, a11, a01, a02, a12, Vf, 0, 1);  // pair (0,1), third index 2
+    jrot_f32(a00, a22, a02, a01, a12, Vf, 0, 2);  // pair (0,2), third index 1
+    jrot_f32(a11, a22, a12, a01, a02, Vf, 1, 2);  // pair (1,2), third index 0
+    const float off = fabsf(a01) + fabsf(a02) + fabsf(a12);
+    if (off <= 1e-7f * (fabsf(a00) + fabsf(a11) + fabsf(a22)) + 1e-30f) break;
+  }
+  // FP64 Gram-Schmidt of the FP32 rotation -> orthonormal V0 (det +1)
+  double v0[3] = {Vf[0], Vf[3], Vf[6]}, v1[3] = {Vf[1], Vf[4], Vf[7]};
+  const double n0 = rsqrt(v0[0] * v0[0] + v0[1] * v0[1] + v0[2] * v0[2]);
+  for (int k = 0; k < 3; ++k) v0[k] *= n0;
+  const double d01 = v0[0] * v1[0] + v0[1] * v1[1] + v0[2] * v1[2];
+  for (int k = 0; k < 3; ++k) v1[k] -= d01 * v0[k];
+  const double n1 = rsqrt(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]);
+  for (int k = 0; k < 3; ++k) v1[k] *= n1;
+  const double v2[3] = {v0[1] * v1[2] - v0[2] * v1[1], v0[2] * v1[0] - v0[0] * v1[2], v0[0] * v1[1] - v0[1] * v1[0]};
+  for (int k = 0; k < 3; ++k) { V[3 * k] = v0[k]; V[3 * k + 1] = v1[k]; V[3 * k + 2] = v2[k]; }
+  double W[9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) W[3 * r + q] = A[3 * r] * V[q] + A[3 * r + 1] * V[3 + q] + A[3 * r + 2] * V[6 + q];
+  const double eps = 2.220446049250313e-16;
+#pragma unroll 1
+  for (int sweep = 0; sweep < 8; ++sweep) {
+    bool rotated = false;
+#pragma unroll
+    for (int pq = 0; pq < 3; ++pq) {
+      const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
+      const double alpha = W[p] * W[p] + W[3 + p] * W[3 + p] + W[6 + p] * W[6 + p];
+      const double beta = W[q] * W[q] + W[3 + q] * W[3 + q] + W[6 + q] * W[6 + q];
+      const double gamma = W[p] * W[q] + W[3 + p] * W[3 + q] + W[6 + p] * W[6 + q];
+      if (gamma == 0.0 || fabs(gamma) <= eps * sqrt(alpha * beta)) continue;
+      rotated = true;
+      const double zeta = (beta - alpha) / (2.0 * gamma);
+      const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+      const double cs = rsqrt(1.0 + t * t);
+      const double sn = cs * t;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double wp = W[3 * k + p], wq = W[3 * k + q];
+        W[3 * k + p] = cs * wp - sn * wq;
+        W[3 * k + q] = sn * wp + cs * wq;
+        const double vp = V[3 * k + p], vq = V[3 * k + q];
+        V[3 * k + p] = cs * vp - sn * vq;
+        V[3 * k + q] = sn * vp + cs * vq;
+      }
+    }
+    if (!rotated) break;
+  }
+  int zero_cols = 0, zc = -1;
+  for (int j = 0; j < 3; ++j) {
+    s[j] = sqrt(W[j] * W[j] + W[3 + j] * W[3 + j] + W[6 + j] * W[6 + j]);
+    if (s[j] > 1e-300) {
+      const double inv = 1.0 / s[j];
+      for (int k = 0; k < 3; ++k) U[3 * k + j] = W[3 * k + j] * inv;
+    } else { ++zero_cols; zc = j; }
+  }
+  if (zero_cols == 1) {
+    const int a = (zc + 1) % 3, b = (zc + 2) % 3;
     U[0 + zc] = U[3 + a] * U[6 + b] - U[6 + a] * U[3 + b];
     U[3 + zc] = U[6 + a] * U[0 + b] - U[0 + a] * U[6 + b];
     U[6 + zc] = U[0 + a] * U[3 + b] - U[3 + a] * U[0 + b];
@@ -1184,7 +1335,7 @@ __device__ void return_map(const Params& P, double dt, const double sg[3], float
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_defgrad(Params P, Bufs B) {
+__global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) {
   const Ctrl* c = B.ctrl;
   if (c->halt) return;
   const int S = P.np_stride, np = P.np;
@@ -1246,7 +1397,7 @@ __global__ void __launch_bounds__(kThreads) k_defgrad(Params P, Bufs B) {
             gv[0] = m.x * inv; gv[1] = m.y * inv; gv[2] = m.z * inv;
           } else {
             const float4 m = B.grid[(size_t)node * 4];
-            gv[0] = m.y; gv[1] = m.z; gv[2] = m.w;
+            gv[0] = m.x; gv[1] = m.y; gv[2] = m.z;
           }
           const float g[3] = {aw[0].dN[a] * aw[1].N[bb] * aw[2].N[cc], aw[0].N[a] * aw[1].dN[bb] * aw[2].N[cc],
                               aw[0].N[a] * aw[1].N[bb] * aw[2].dN[cc]};
@@ -1270,7 +1421,7 @@ __global__ void __launch_bounds__(kThreads) k_defgrad(Params P, Bufs B) {
       }
     float epd = pi[F_EPD * S + o], epv = pi[F_EPV * S + o], epp = pi[F_EPP * S + o], dgam = 0.f;
     double U[9], V[9], sg[3];
-    svd3_d(Ft, U, sg, V);
+    svd3_warm(Ft, U, sg, V);
     double hfin[3];
     float Fout[9];
     bool changed = false;
