@@ -158,16 +158,50 @@ PM_API pm_status pm_get_stats(pm_sim* sim, double* total_mass, double momentum[3
 PM_API pm_status pm_get_grid(pm_sim* sim, double origin[3], uint32_t dims[3], float* mass, float* v_update,
                       float* v_musl, float* flip, float* latent, float* shear);
 
-/* ---- learned return map (no reference counterpart) ----------------------------------------- */
-/* Selects the return-map implementation used by pm_step/pm_advance. */
+/* ---- learned return map (no reference counterpart) -----------------------------------------
+ * A 10 -> 64 -> 64 -> 6 GELU MLP predicts the viscoplastic projection of the Perzyna return map
+ * (plasticity.cpp:194-229 VMVisc, :292-325 DPVisc) for particles that would need the Newton
+ * solve.  Features: trial principal log strains (3), deviatoric strain rate dev(h)/dt (3), yield
+ * stress, Perzyna viscosity, flow index, Young's modulus.  Targets: plastic strain h_trial - h (3)
+ * and its rate (3).  Parameter vector (PM_MLP_NPARAMS floats): in_mean[10] in_std[10]
+ * out_mean[6] out_std[6] W1[64][10] b1[64] W2[64][64] b2[64] W3[6][64] b3[6]. */
+#define PM_MLP_NPARAMS 5286
+/* Selects the return-map implementation used by pm_step/pm_advance: PM_RETURN_MAP_SURROGATE
+ * needs weights from pm_set_surrogate.  Every surrogate estimate is checked against the Perzyna
+ * consistency condition (|r| < 1e-2 Pa, the reference's tolerance); estimates that fail drop to
+ * the Newton solve (continued from the estimate, or from the reference's initial guess when the
+ * parameter "surrogate_fallback_plain" is 1). */
 PM_API pm_status pm_set_return_map(pm_sim* sim, int mode);
+/* Loads surrogate weights (host array, PM_MLP_NPARAMS floats) for BF16 tensor-core inference. */
+PM_API pm_status pm_set_surrogate(pm_sim* sim, const float* params);
+/* Turns on logging of (features, targets) for every particle the plain return map solves with
+ * Newton, up to `capacity` samples (0 turns it off; the buffer is device memory). */
+PM_API pm_status pm_enable_sample_log(pm_sim* sim, uint32_t capacity);
+/* Copies up to max_samples logged samples: features[n*10], targets[n*6]; *n = number copied. */
+PM_API pm_status pm_get_samples(pm_sim* sim, float* features, float* targets, uint32_t max_samples, uint32_t* n);
+/* Return-map statistics of the last step: [0] particles needing the consistency solve,
+ * [1] Newton updates taken, [2] particles sent to the surrogate, [3] surrogate estimates that
+ * passed the check, [4] samples logged so far. */
+PM_API pm_status pm_get_return_map_stats(pm_sim* sim, uint32_t stats[5]);
+/* Trains the MLP on the current device with the library's FP32 forward/backward kernels and
+ * Adam (cosine learning-rate decay).  x[n*10], y[n*6] host arrays; params (in/out) receives the
+ * trained vector (resume = 1 starts from its content, 0 initialises it and the normalisation
+ * statistics from the data); loss_history[epochs] (may be NULL) the mean normalised MSE per epoch. */
+PM_API pm_status pm_mlp_train(const float* x, const float* y, uint32_t n, uint32_t epochs, uint32_t batch, float lr,
+                              uint64_t seed, int resume, float* params, float* loss_history, uint32_t* steps);
+/* Normalised mean-squared-error loss and its gradient (grad[PM_MLP_NPARAMS], statistics entries
+ * zero) of one batch, computed by the training kernels (for gradient checks). */
+PM_API pm_status pm_mlp_loss_grad(const float* params, const float* x, const float* y, uint32_t n, float* loss,
+                                  float* grad);
+/* Inference through the BF16 tensor-core kernel: x[n*10] -> y[n*6], host arrays. */
+PM_API pm_status pm_mlp_infer(const float* params, const float* x, uint32_t n, float* y);
 
 /* ---- diagnostics (no reference counterpart; the reference times phases with gettimeofday,
  * simulation.cpp:247-274) -------------------------------------------------------------------- */
 /* The cudaStream_t all of this simulation's work is issued on (for CUDA event timing). */
 PM_API pm_status pm_get_stream(pm_sim* sim, void** stream);
-/* Name of the i-th kernel of a step (launch order), "" when out of range. */
-PM_API const char* pm_kernel_name(int index);
+/* Name of the i-th kernel of this simulation's step (launch order), "" when out of range. */
+PM_API const char* pm_kernel_name(pm_sim* sim, int index);
 /* Runs nsteps ordinary steps (no graph), timing every kernel with CUDA events on the stream;
  * kernel_ms[i] receives the mean duration of kernel i.  n_kernels must be >= the kernels per
  * step (pm_get_param "kernels_per_step"). */

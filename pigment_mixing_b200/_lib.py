@@ -50,6 +50,13 @@ SIGNATURES = {
     "pm_set_return_map": [_vp, C.c_int],
     "pm_get_stream": [_vp, C.POINTER(C.c_void_p)],
     "pm_profile_steps": [_vp, C.c_uint32, _fp, C.c_uint32],
+    "pm_set_surrogate": [_vp, _fp],
+    "pm_enable_sample_log": [_vp, C.c_uint32],
+    "pm_get_samples": [_vp, _fp, _fp, C.c_uint32, _up],
+    "pm_get_return_map_stats": [_vp, _up],
+    "pm_mlp_train": [_fp, _fp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64, C.c_int, _fp, _fp, _up],
+    "pm_mlp_loss_grad": [_fp, _fp, _fp, C.c_uint32, _fp, _fp],
+    "pm_mlp_infer": [_fp, _fp, C.c_uint32, _fp],
     "pm_p2g_noalloc": [_vp] * 5 + [C.c_uint32, C.c_double, C.c_double, _dp, C.POINTER(C.c_int32)] + [_vp] * 5 + [_up],
 }
 
@@ -77,7 +84,7 @@ def lib() -> C.CDLL:
     L.pm_last_error_message.restype = C.c_char_p
     L.pm_last_error_message.argtypes = []
     L.pm_kernel_name.restype = C.c_char_p
-    L.pm_kernel_name.argtypes = [C.c_int]
+    L.pm_kernel_name.argtypes = [C.c_void_p, C.c_int]
     _lib = L
     return L
 

@@ -17,6 +17,7 @@
 #include "../../include/pigment_mpm.h"
 #include "pm_internal.cuh"
 #include "pm_launch.h"
+#include "pm_mlp.h"
 
 using namespace pm;
 
@@ -121,7 +122,16 @@ struct pm_sim {
   float* d_unperm = nullptr;
   uint8_t* d_active = nullptr;
   double* d_stats = nullptr;
-  void* d_mlp = nullptr;
+  void* d_mlp = nullptr;       // inference weights (bf16 matrices, FP32 biases and statistics)
+  MlpDev mlp_dev{};
+  bool has_mlp = false;
+  int sur_fallback_plain = 0;
+  float* d_slog = nullptr;     // return-map sample log: log_cap x 16 floats
+  uint32_t log_cap = 0;
+  SurQ* d_q = nullptr;         // surrogate queue (q_cap records + inputs and outputs)
+  float* d_qx = nullptr;
+  float* d_qy = nullptr;
+  uint32_t q_cap = 0;
 
   bool prepared = false;
   uint32_t host_step = 0;  // steps completed (mirror of ctrl.step after the last sync)
@@ -140,6 +150,8 @@ struct pm_sim {
   pm_status run_steps(uint32_t n, bool use_graph);
   pm_status capture_graphs();
   void drop_graphs();
+  void free_surrogate_queue();
+  pm_status ensure_surrogate_queue();
 };
 
 pm_sim::~pm_sim() {
@@ -151,7 +163,29 @@ pm_sim::~pm_sim() {
   if (d_frames) cudaFree(d_frames);
   if (d_stats) cudaFree(d_stats);
   if (d_mlp) cudaFree(d_mlp);
+  if (d_slog) cudaFree(d_slog);
+  free_surrogate_queue();
   if (stream) cudaStreamDestroy(stream);
+}
+
+void pm_sim::free_surrogate_queue() {
+  if (d_q) cudaFree(d_q);
+  if (d_qx) cudaFree(d_qx);
+  if (d_qy) cudaFree(d_qy);
+  d_q = nullptr; d_qx = nullptr; d_qy = nullptr;
+  q_cap = 0;
+}
+
+pm_status pm_sim::ensure_surrogate_queue() {
+  const uint32_t want = (uint32_t)std::max(np_stride, 32);
+  if (q_cap >= want && d_q) return PM_OK;
+  drop_graphs();
+  free_surrogate_queue();
+  CK(cudaMalloc(&d_q, (size_t)want * sizeof(SurQ)));
+  CK(cudaMalloc(&d_qx, (size_t)want * 10 * sizeof(float)));
+  CK(cudaMalloc(&d_qy, (size_t)want * 6 * sizeof(float)));
+  q_cap = want;
+  return PM_OK;
 }
 
 void pm_sim::drop_graphs() {
@@ -215,7 +249,11 @@ Bufs pm_sim::bufs(int parity) const {
   b.grid = d_grid;
   b.gmusl = d_gmusl;
   b.ctrl = d_ctrl;
-  b.mlp = d_mlp;
+  b.mlp = mlp_dev;
+  b.slog = d_slog;
+  b.q = d_q;
+  b.qx = d_qx;
+  b.qy = d_qy;
   return b;
 }
 
@@ -244,6 +282,7 @@ void pm_sim::fill_params() {
   p.lambda = h.nu * h.E / ((1.0 + h.nu) * (1.0 - 2.0 * h.nu));
   p.mu = h.E / (2.0 * (1.0 + h.nu));
   p.K = p.lambda + 2.0 * p.mu / 3.0;
+  p.E = h.E;
   p.d_prefac = 1.0 / h.q_prefac;
   p.e_mu_prefac = 2.0 * h.q_prefac * p.mu;
   p.f_mu_prefac = 2.0 * h.q_prefac * h.q_prefac * p.mu;
@@ -263,7 +302,10 @@ void pm_sim::fill_params() {
   p.node_cap = brick_cap * kBrickNodes;
   p.frames = d_frames;
   p.n_frames = (int)(frames.size() / 7);
-  p.return_map = return_map;
+  p.return_map = (return_map == PM_RETURN_MAP_SURROGATE && has_mlp && d_q) ? 1 : 0;
+  p.sur_fallback_plain = sur_fallback_plain;
+  p.log_cap = d_slog ? log_cap : 0;
+  p.q_cap = d_q ? q_cap : 0;
   graphs_dirty = true;
 }
 
@@ -283,8 +325,8 @@ pm_status pm_sim::capture_graphs() {
   for (int start = 0; start < 2; ++start) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    launch_step(P, bufs(start), stream);
-    launch_step(P, bufs(start ^ 1), stream);
+    launch_step(P, bufs(start), stream, nullptr);
+    launch_step(P, bufs(start ^ 1), stream, nullptr);
     cudaError_t e = cudaStreamEndCapture(stream, &g);
     if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     e = cudaGraphInstantiate(&gexec[start], g, 0);
@@ -308,7 +350,7 @@ pm_status pm_sim::run_steps(uint32_t n, bool use_graph) {
       for (; k + 2 <= remaining; k += 2) CK(cudaGraphLaunch(gexec[par], stream));
     }
     int par = (cur + (int)k) & 1;
-    for (; k < remaining; ++k) { launch_step(P, bufs(par), stream); par ^= 1; }
+    for (; k < remaining; ++k) { launch_step(P, bufs(par), stream, nullptr); par ^= 1; }
     CK(cudaGetLastError());
     pm_status s = sync_ctrl();
     if (s != PM_OK) return s;
@@ -423,6 +465,7 @@ pm_status pm_set_param(pm_sim* sim, const char* name, double v) {
   } else if (k == "end_frame") { h.end_frame = v; ctrl_field = true; }
   else if (k == "frame") { ctrl_field = true; }
   else if (k == "auto_frame") { h.auto_frame = v != 0; ctrl_field = true; }
+  else if (k == "surrogate_fallback_plain") { sim->sur_fallback_plain = v != 0; }
   else return fail(PM_ERR_INVALID, "unknown parameter " + k);
   if (sim->prepared) {
     if (k == "dx") return fail(PM_ERR_STATE, "dx cannot change after prepare");
@@ -457,7 +500,8 @@ pm_status pm_get_param(pm_sim* sim, const char* name, double* out) {
   else if (k == "n_active") *out = c->n_active;
   else if (k == "plastic_count") *out = c->plastic_count;
   else if (k == "grid_nodes") *out = c->n_nodes;
-  else if (k == "kernels_per_step") *out = kernels_per_step();
+  else if (k == "kernels_per_step") *out = kernels_per_step(sim->P);
+  else if (k == "surrogate_fallback_plain") *out = sim->sur_fallback_plain;
   else if (k == "Np") *out = sim->np;
   else if (k == "fps") *out = h.fps;
   else if (k == "cfl") *out = h.cfl;
@@ -571,6 +615,7 @@ pm_status pm_set_particles(pm_sim* sim, uint32_t n, const float* x, const float*
   cudaSetDevice(sim->device);
   sim->drop_graphs();
   sim->free_particles();
+  sim->free_surrogate_queue();
   sim->np = n;
   sim->np_stride = (int)((n + 31) / 32 * 32);
   const size_t S = (size_t)std::max(sim->np_stride, 32);
@@ -852,6 +897,7 @@ pm_status pm_prepare(pm_sim* sim) {
       if ((s = sim->alloc_grid((int)want)) != PM_OK) return s;
     }
   }
+  if (sim->return_map == PM_RETURN_MAP_SURROGATE && (s = sim->ensure_surrogate_queue()) != PM_OK) return s;
   sim->prepared = true;
   sim->fill_params();
   if ((s = sim->push_ctrl()) != PM_OK) return s;
@@ -1028,10 +1074,116 @@ pm_status pm_get_grid(pm_sim* sim, double origin[3], uint32_t dims[3], float* ma
 pm_status pm_set_return_map(pm_sim* sim, int mode) {
   if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
   if (mode != PM_RETURN_MAP_PLAIN && mode != PM_RETURN_MAP_SURROGATE) return fail(PM_ERR_INVALID, "mode");
-  if (mode == PM_RETURN_MAP_SURROGATE && !sim->d_mlp)
-    return fail(PM_ERR_STATE, "no surrogate weights loaded");
+  if (mode == PM_RETURN_MAP_SURROGATE && !sim->has_mlp) return fail(PM_ERR_STATE, "no surrogate weights loaded");
+  CK(cudaSetDevice(sim->device));
   sim->return_map = mode;
+  if (mode == PM_RETURN_MAP_SURROGATE && sim->np > 0) {
+    pm_status s = sim->ensure_surrogate_queue();
+    if (s != PM_OK) return s;
+  }
   if (sim->prepared) sim->fill_params();
+  return PM_OK;
+}
+
+pm_status pm_set_surrogate(pm_sim* sim, const float* params) {
+  if (!sim || !params) return fail(PM_ERR_INVALID, "NULL argument");
+  CK(cudaSetDevice(sim->device));
+  CK(mlp_upload(params, sim->mlp_dev, &sim->d_mlp));
+  sim->has_mlp = true;
+  sim->drop_graphs();
+  if (sim->prepared) sim->fill_params();
+  return PM_OK;
+}
+
+pm_status pm_enable_sample_log(pm_sim* sim, uint32_t capacity) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  CK(cudaSetDevice(sim->device));
+  sim->drop_graphs();
+  if (sim->d_slog) { cudaFree(sim->d_slog); sim->d_slog = nullptr; }
+  sim->log_cap = 0;
+  if (capacity > 0) {
+    CK(cudaMalloc(&sim->d_slog, (size_t)capacity * 16 * sizeof(float)));
+    sim->log_cap = capacity;
+  }
+  if (sim->prepared) {
+    pm_status s = sim->sync_ctrl();
+    if (s != PM_OK) return s;
+    sim->h_ctrl->slog_n = 0;
+    if ((s = sim->push_ctrl()) != PM_OK) return s;
+    sim->fill_params();
+  } else {
+    sim->h_ctrl->slog_n = 0;
+  }
+  return PM_OK;
+}
+
+pm_status pm_get_samples(pm_sim* sim, float* features, float* targets, uint32_t max_samples, uint32_t* n) {
+  if (!sim || !n) return fail(PM_ERR_INVALID, "NULL argument");
+  *n = 0;
+  if (!sim->d_slog) return PM_OK;
+  pm_status s = sim->sync_ctrl();
+  if (s != PM_OK) return s;
+  const uint32_t have = std::min(sim->h_ctrl->slog_n, sim->log_cap);
+  const uint32_t m = std::min(have, max_samples);
+  if (m > 0 && (features || targets)) {
+    std::vector<float> tmp((size_t)m * 16);
+    CK(cudaMemcpy(tmp.data(), sim->d_slog, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (uint32_t r = 0; r < m; ++r) {
+      if (features) std::memcpy(features + (size_t)r * 10, &tmp[(size_t)r * 16], 10 * sizeof(float));
+      if (targets) std::memcpy(targets + (size_t)r * 6, &tmp[(size_t)r * 16 + 10], 6 * sizeof(float));
+    }
+  }
+  *n = m;
+  return PM_OK;
+}
+
+pm_status pm_get_return_map_stats(pm_sim* sim, uint32_t stats[5]) {
+  if (!sim || !stats) return fail(PM_ERR_INVALID, "NULL argument");
+  pm_status s = sim->sync_ctrl();
+  if (s != PM_OK) return s;
+  const Ctrl* c = sim->h_ctrl;
+  stats[0] = c->newton_solves;
+  stats[1] = c->newton_iters;
+  stats[2] = c->q_n;
+  stats[3] = c->sur_accept;
+  stats[4] = c->slog_n;
+  return PM_OK;
+}
+
+pm_status pm_mlp_loss_grad(const float* params, const float* x, const float* y, uint32_t n, float* loss, float* grad) {
+  if (!params || !x || !y || !loss || n == 0) return fail(PM_ERR_INVALID, "NULL argument or empty batch");
+  CK(mlp_loss_grad(params, x, y, (int)n, loss, grad));
+  return PM_OK;
+}
+
+pm_status pm_mlp_train(const float* x, const float* y, uint32_t n, uint32_t epochs, uint32_t batch, float lr,
+                       uint64_t seed, int resume, float* params, float* loss_history, uint32_t* steps) {
+  if (!x || !y || !params || n == 0) return fail(PM_ERR_INVALID, "NULL argument or empty training set");
+  pm_mlp_train_opts o{(int)epochs, (int)batch, lr, seed, resume};
+  int st = 0;
+  CK(mlp_train(x, y, (int)n, o, params, loss_history, &st));
+  if (steps) *steps = (uint32_t)st;
+  return PM_OK;
+}
+
+pm_status pm_mlp_infer(const float* params, const float* x, uint32_t n, float* y) {
+  if (!params || !x || !y) return fail(PM_ERR_INVALID, "NULL argument");
+  if (n == 0) return PM_OK;
+  void* storage = nullptr;
+  MlpDev dev{};
+  float* dX = nullptr;
+  float* dY = nullptr;
+  cudaError_t e = mlp_upload(params, dev, &storage);
+  if (e == cudaSuccess) e = cudaMalloc(&dX, (size_t)n * 10 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dY, (size_t)n * 6 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpy(dX, x, (size_t)n * 10 * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = mlp_init();
+  if (e == cudaSuccess) e = mlp_infer(dev, dX, dY, (int)n, nullptr, 0, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(y, dY, (size_t)n * 6 * sizeof(float), cudaMemcpyDeviceToHost);
+  if (dX) cudaFree(dX);
+  if (dY) cudaFree(dY);
+  if (storage) cudaFree(storage);
+  if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("pm_mlp_infer: ") + cudaGetErrorString(e));
   return PM_OK;
 }
 
@@ -1041,21 +1193,21 @@ pm_status pm_get_stream(pm_sim* sim, void** stream) {
   return PM_OK;
 }
 
-const char* pm_kernel_name(int index) { return kernel_name(index); }
+const char* pm_kernel_name(pm_sim* sim, int index) { return sim ? kernel_name(index, sim->P) : ""; }
 
 pm_status pm_profile_steps(pm_sim* sim, uint32_t nsteps, float* kernel_ms, uint32_t n_kernels) {
   if (!sim || !kernel_ms) return fail(PM_ERR_INVALID, "NULL argument");
   if (!sim->prepared) return fail(PM_ERR_STATE, "call pm_prepare first");
-  const int K = kernels_per_step();
+  const int K = kernels_per_step(sim->P);
   if ((int)n_kernels < K) return fail(PM_ERR_INVALID, "kernel_ms needs kernels_per_step entries");
   CK(cudaSetDevice(sim->device));
-  std::vector<cudaEvent_t> ev(13);
+  std::vector<cudaEvent_t> ev(K + 1);
   for (auto& e : ev) CK(cudaEventCreate(&e));
   std::vector<double> acc(K, 0.0);
   uint32_t done_steps = 0;
   pm_status st = PM_OK;
   for (uint32_t k = 0; k < nsteps && st == PM_OK; ++k) {
-    launch_step_timed(sim->P, sim->bufs(sim->cur), sim->stream, ev.data());
+    launch_step(sim->P, sim->bufs(sim->cur), sim->stream, ev.data());
     if (cudaStreamSynchronize(sim->stream) != cudaSuccess) { st = fail(PM_ERR_CUDA, "profiled step failed"); break; }
     for (int i = 0; i < K; ++i) {
       float ms = 0.f;

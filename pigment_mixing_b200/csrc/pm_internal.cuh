@@ -16,6 +16,8 @@
 #include <cstdint>
 #include <cstring>
 
+#include "pm_mlp.h"
+
 namespace pm {
 
 constexpr int kMaxPlates = 8;
@@ -104,6 +106,7 @@ struct Params {
   float pbmin[3], pbmax[3];
   // material
   double mu, lambda, K;
+  double E;               // Young's modulus (a surrogate feature)
   double e_mu_prefac, f_mu_prefac, d_prefac;
   double q_max, q_min, p_min, M, q_cohesion, perzyna_exp, perzyna_visc, xi;
   int plastic_model;
@@ -119,6 +122,20 @@ struct Params {
   const float* frames;
   int n_frames;
   int return_map;         // 0 plain, 1 surrogate
+  int sur_fallback_plain; // surrogate mode: 1 = failed checks restart Newton from the reference guess
+  uint32_t log_cap;       // capacity of the return-map sample log (0 = off)
+  uint32_t q_cap;         // capacity of the surrogate queue
+};
+
+// One particle waiting for the surrogate (the state the return map needs to finish).
+struct SurQ {
+  double U[9], V[9];
+  double h[3], hd[3];     // clamped principal log strains, unit deviatoric direction
+  double q_trial, q_y;
+  float epd;
+  uint32_t i;             // particle slot (sorted order)
+  uint32_t vm;            // 1 VMVisc, 0 DPVisc
+  uint32_t pad;
 };
 
 struct Ctrl {
@@ -142,7 +159,12 @@ struct Ctrl {
   int xmin_key[3], xmax_key[3];
   uint32_t n_active;
   uint32_t plastic_count;
-  uint32_t surrogate_fallbacks;
+  // return-map statistics of the last step and the sample log fill
+  uint32_t q_n;            // particles queued for the surrogate this step
+  uint32_t newton_iters;   // Newton updates this step
+  uint32_t newton_solves;  // particles that needed the Perzyna consistency solve this step
+  uint32_t sur_accept;     // surrogate estimates that passed the consistency check
+  uint32_t slog_n;         // samples written to the log (cumulative)
   uint32_t pad0;
   // objects
   int n_plates, n_objects, knife;  // knife: index into objects or -1
@@ -166,7 +188,11 @@ struct Bufs {
   float4* gmusl;          // node_cap float4
   Ctrl* ctrl;
   // learned return map (optional)
-  const void* mlp;
+  MlpDev mlp;
+  float* slog;            // log_cap x 16: features[10], targets[6]
+  SurQ* q;                // q_cap records
+  float* qx;              // q_cap x 10 surrogate inputs
+  float* qy;              // q_cap x 6 surrogate outputs
 };
 
 // Order-preserving float <-> int key (min/max of floats through integer atomics).

@@ -152,6 +152,10 @@ __global__ void k_prologue(Params P, Bufs B) {
   for (int d = 0; d < 3; ++d) { c->xmin_key[d] = 0x7fffffff; c->xmax_key[d] = (int)0x80000000; }
   c->n_active = 0;
   c->plastic_count = 0;
+  c->q_n = 0;
+  c->newton_iters = 0;
+  c->newton_solves = 0;
+  c->sur_accept = 0;
 }
 
 // quaternion helpers (w, x, y, z)
@@ -1228,27 +1232,105 @@ struct ReturnMapOut {
   double h[3];       // final principal log strains
   bool changed;      // F replaced by U exp(h) V^T
   bool to_rotation;  // capped VM branch: F = U V^T
+  bool queued;       // surrogate mode: the consistency solve is left to the surrogate pass
 };
 
+// Perzyna consistency solve (plasticity.cpp:194-229 VMVisc, :292-325 DPVisc): Newton on
+// r(dg) = (q_trial - f dg) (dt / (eta dg + dt))^m - q_yield(dg) from dg until |r| < 1e-2, at most
+// 60 iterations.  iters counts the Newton updates taken.
+__device__ double perzyna_newton(const Params& P, bool vm, double q_trial, double q_yield_dp, double epd, double dt,
+                                 double dg, uint32_t& iters, uint32_t& err) {
+  const double fmu = P.f_mu_prefac, dpre = P.d_prefac;
+  for (int it = 0; it < 60; ++it) {
+    if (it == 59) err |= E_NEWTON_NOCONV;
+    const double tm = P.perzyna_visc * dg + dt;
+    const double tmp = dt / tm;
+    const double tmp1 = exp(P.perzyna_exp * log(tmp));  // tmp^m; tmp^(m-1) = tmp1 / tmp
+    const double tmpm1 = tmp1 / tmp;
+    const double q_yield = vm ? P.q_min + (P.q_max - P.q_min) * exp(-P.xi * (epd + dg / dpre)) : q_yield_dp;
+    const double res = (q_trial - fmu * dg) * tmp1 - q_yield;
+    if (fabs(res) < 1e-2) break;
+    const double qyd = vm ? -P.xi / dpre * (P.q_max - P.q_min) * exp(-P.xi * (epd + dg / dpre)) : 0.0;
+    const double rd = -fmu * tmp1 + (q_trial - fmu * dg) * P.perzyna_exp * tmpm1 * (-P.perzyna_visc * dt) / (tm * tm) - qyd;
+    if (fabs(rd) < 1e-14) err |= E_NEWTON_FLAT;
+    dg -= res / rd;
+    if (dg < 0) dg = 1e-10;
+    ++iters;
+  }
+  return dg;
+}
+
+// Surrogate features of a particle on the Newton path: trial log strains, deviatoric strain
+// rate, yield, viscosity, flow index, Young's modulus.
+__device__ __forceinline__ void sur_features(const Params& P, const double h[3], double dt, double q_yield, float f[10]) {
+  const double m = (h[0] + h[1] + h[2]) / 3.0;
+  for (int k = 0; k < 3; ++k) { f[k] = (float)h[k]; f[3 + k] = (float)((h[k] - m) / dt); }
+  f[6] = (float)q_yield;
+  f[7] = (float)P.perzyna_visc;
+  f[8] = (float)P.perzyna_exp;
+  f[9] = (float)P.E;
+}
+
+// The Newton path of the return map: either queue the particle for the surrogate, or solve
+// (and, when the sample log is on, record features and the projected strains).
+__device__ bool newton_path(const Params& P, const Bufs& B, uint32_t i, bool vm, double dt, const double h[3],
+                            const double hd[3], double q_trial, double q_yield, float epd, const double* U,
+                            const double* V, double& dg, uint32_t& iters, uint32_t& err) {
+  if (P.return_map == 1 && P.q_cap > 0) {
+    const uint32_t slot = atomicAdd(&B.ctrl->q_n, 1u);
+    if (slot < P.q_cap) {
+      SurQ& r = B.q[slot];
+      for (int k = 0; k < 9; ++k) { r.U[k] = U[k]; r.V[k] = V[k]; }
+      for (int k = 0; k < 3; ++k) { r.h[k] = h[k]; r.hd[k] = hd[k]; }
+      r.q_trial = q_trial;
+      r.q_y = q_yield;
+      r.epd = epd;
+      r.i = i;
+      r.vm = vm ? 1u : 0u;
+      float f[10];
+      sur_features(P, h, dt, q_yield, f);
+      for (int k = 0; k < 10; ++k) B.qx[(size_t)slot * 10 + k] = f[k];
+      return true;
+    }
+    err |= E_CAPACITY;  // queue full: solve here
+  }
+  dg = perzyna_newton(P, vm, q_trial, q_yield, (double)epd, dt, 0.01 * (q_trial - q_yield) / P.f_mu_prefac, iters, err);
+  if (P.log_cap > 0) {
+    const uint32_t slot = atomicAdd(&B.ctrl->slog_n, 1u);
+    if (slot < P.log_cap) {
+      float* o = B.slog + (size_t)slot * 16;
+      sur_features(P, h, dt, q_yield, o);
+      for (int k = 0; k < 3; ++k) {
+        const double d = (dg / P.d_prefac) * hd[k];  // h - h_projected
+        o[10 + k] = (float)d;
+        o[13 + k] = (float)(d / dt);
+      }
+    }
+  }
+  return false;
+}
+
 // plasticity.cpp:163-238 (VMVisc) and :240-340 (DPVisc) in FP64
-__device__ void return_map(const Params& P, double dt, const double sg[3], float& epd, float& epv, float& epp, float& dgam,
-                           uint32_t& plastic, uint32_t& err, ReturnMapOut& out) {
+__device__ void return_map(const Params& P, const Bufs& B, uint32_t i, double dt, const double sg[3], const double* U,
+                           const double* V, float& epd, float& epv, float& epp, float& dgam, uint32_t& plastic,
+                           uint32_t& iters, uint32_t& solves, uint32_t& err, ReturnMapOut& out) {
   double h[3];
-  for (int i = 0; i < 3; ++i) h[i] = log(fmax(fabs(sg[i]), 1e-4));
+  for (int k = 0; k < 3; ++k) h[k] = log(fmax(fabs(sg[k]), 1e-4));
   const double htr = h[0] + h[1] + h[2];
   double hd[3] = {h[0] - htr / 3.0, h[1] - htr / 3.0, h[2] - htr / 3.0};
   const double hdn = sqrt(hd[0] * hd[0] + hd[1] * hd[1] + hd[2] * hd[2]);
-  if (hdn > 0) for (int i = 0; i < 3; ++i) hd[i] /= hdn;
+  if (hdn > 0) for (int k = 0; k < 3; ++k) hd[k] /= hdn;
   out.changed = false;
   out.to_rotation = false;
-  for (int i = 0; i < 3; ++i) out.h[i] = h[i];
+  out.queued = false;
+  for (int k = 0; k < 3; ++k) out.h[k] = h[k];
   const double fmu = P.f_mu_prefac, emu = P.e_mu_prefac, dpre = P.d_prefac;
   if (P.plastic_model == PL_VMVISC) {
     const double q_trial = emu * hdn;
     double q_yield = P.q_min + (P.q_max - P.q_min) * exp(-P.xi * (double)epd);
     const double p_trial = -P.K * htr;
     if (p_trial < P.p_min * exp(-P.xi * (double)epv)) {
-      double dg = q_trial / fmu;
+      const double dg = q_trial / fmu;
       out.to_rotation = true;
       out.changed = true;
       epv = (float)((double)epv + (-p_trial / P.K));
@@ -1256,30 +1338,15 @@ __device__ void return_map(const Params& P, double dt, const double sg[3], float
       dgam = (float)(dg / dt);
     } else if (q_trial > q_yield) {
       ++plastic;
-      double dg;
+      double dg = 0.0;
       if (P.perzyna_exp == 1.0 && P.xi == 0.0) {
         dg = (q_trial - q_yield) / (fmu + q_yield * P.perzyna_visc / dt);
         if (dg < 0) err |= E_NEG_DGAMMA;
       } else {
-        dg = 0.01 * (q_trial - q_yield) / fmu;
-        for (int it = 0; it < 60; ++it) {
-          if (it == 59) err |= E_NEWTON_NOCONV;
-          double tm = P.perzyna_visc * dg + dt;
-          double tmp = dt / tm;
-          // tmp^m and tmp^(m-1) = tmp^m / tmp from one log and one exp
-          double tmp1 = exp(P.perzyna_exp * log(tmp));
-          double tmpm1 = tmp1 / tmp;
-          q_yield = P.q_min + (P.q_max - P.q_min) * exp(-P.xi * ((double)epd + dg / dpre));
-          double res = (q_trial - fmu * dg) * tmp1 - q_yield;
-          if (fabs(res) < 1e-2) break;
-          double qyd = -P.xi / dpre * (P.q_max - P.q_min) * exp(-P.xi * ((double)epd + dg / dpre));
-          double rd = -fmu * tmp1 + (q_trial - fmu * dg) * P.perzyna_exp * tmpm1 * (-P.perzyna_visc * dt) / (tm * tm) - qyd;
-          if (fabs(rd) < 1e-14) err |= E_NEWTON_FLAT;
-          dg -= res / rd;
-          if (dg < 0) dg = 1e-10;
-        }
+        ++solves;
+        if (newton_path(P, B, i, true, dt, h, hd, q_trial, q_yield, epd, U, V, dg, iters, err)) { out.queued = true; return; }
       }
-      for (int i = 0; i < 3; ++i) out.h[i] = h[i] - (dg / dpre) * hd[i];
+      for (int k = 0; k < 3; ++k) out.h[k] = h[k] - (dg / dpre) * hd[k];
       out.changed = true;
       epd = (float)((double)epd + dg / dpre);
       dgam = (float)(dg / dt);
@@ -1295,7 +1362,7 @@ __device__ void return_map(const Params& P, double dt, const double sg[3], float
       const double epv_inst = (p_tip - p_trial) / P.K;
       ++plastic;
       const double hh = -p_tip / (P.K * 3.0);
-      for (int i = 0; i < 3; ++i) out.h[i] = hh;
+      for (int k = 0; k < 3; ++k) out.h[k] = hh;
       out.changed = true;
       dgam = (float)(dg / dt);
       epd = (float)((double)epd + dg / dpre);
@@ -1307,32 +1374,44 @@ __device__ void return_map(const Params& P, double dt, const double sg[3], float
     }
     if ((p_trial + p_shift) > p_tip && q_trial > q_yield) {
       ++plastic;
-      double dg;
+      double dg = 0.0;
       if (P.perzyna_exp == 1.0) {
         dg = (q_trial - q_yield) / (fmu + q_yield * P.perzyna_visc / dt);
         if (dg < 0) err |= E_NEG_DGAMMA;
       } else {
-        dg = 0.01 * (q_trial - q_yield) / fmu;
-        for (int it = 0; it < 60; ++it) {
-          if (it == 59) err |= E_NEWTON_NOCONV;
-          double tm = P.perzyna_visc * dg + dt;
-          double tmp = dt / tm;
-          double tmp1 = exp(P.perzyna_exp * log(tmp));
-          double tmpm1 = tmp1 / tmp;
-          double res = (q_trial - fmu * dg) * tmp1 - q_yield;
-          if (fabs(res) < 1e-2) break;
-          double rd = -fmu * tmp1 + (q_trial - fmu * dg) * P.perzyna_exp * tmpm1 * (-P.perzyna_visc * dt) / (tm * tm);
-          if (fabs(rd) < 1e-14) err |= E_NEWTON_FLAT;
-          dg -= res / rd;
-          if (dg < 0) dg = 1e-10;
-        }
+        ++solves;
+        if (newton_path(P, B, i, false, dt, h, hd, q_trial, q_yield, epd, U, V, dg, iters, err)) { out.queued = true; return; }
       }
-      for (int i = 0; i < 3; ++i) out.h[i] = h[i] - (dg / dpre) * hd[i];
+      for (int k = 0; k < 3; ++k) out.h[k] = h[k] - (dg / dpre) * hd[k];
       out.changed = true;
       epd = (float)((double)epd + dg / dpre);
       dgam = (float)(dg / dt);
     }
   }
+}
+
+// F = U exp(h) V^T and the Kirchhoff stress tau = U diag(2 mu h + lambda tr h) U^T of the final F
+// (simulation.hpp:287-294 evaluated on the factors the return map already has).
+__device__ __forceinline__ void finish_F_tau(const Params& P, const double* U, const double* V, const double hfin[3],
+                                             bool rebuild, const double* Ft, float Fout[9], float tau[6]) {
+  if (rebuild) {
+    const double e[3] = {exp(hfin[0]), exp(hfin[1]), exp(hfin[2])};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        Fout[3 * r + q] = (float)(U[3 * r] * e[0] * V[3 * q] + U[3 * r + 1] * e[1] * V[3 * q + 1] + U[3 * r + 2] * e[2] * V[3 * q + 2]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Fout[k] = (float)Ft[k];
+  }
+  const double tr = hfin[0] + hfin[1] + hfin[2];
+  double d[3];
+  for (int k = 0; k < 3; ++k) d[k] = 2.0 * P.mu * hfin[k] + P.lambda * tr;
+  if (!(isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2]))) { d[0] = d[1] = d[2] = 0.0; }
+  auto T = [&](int r, int q) { return U[3 * r] * d[0] * U[3 * q] + U[3 * r + 1] * d[1] * U[3 * q + 1] + U[3 * r + 2] * d[2] * U[3 * q + 2]; };
+  tau[0] = (float)T(0, 0); tau[1] = (float)T(1, 1); tau[2] = (float)T(2, 2);
+  tau[3] = (float)T(0, 1); tau[4] = (float)T(0, 2); tau[5] = (float)T(1, 2);
 }
 
 __global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) {
@@ -1342,7 +1421,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) {
   const double dt = c->dt;
   const float dtf = (float)dt;
   const float dx = P.dx;
-  uint32_t err = 0, plastic = 0, nact = 0;
+  uint32_t err = 0, plastic = 0, nact = 0, niters = 0, nsolves = 0;
   float maxv2 = 0.f;
   int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
   const int stride = gridDim.x * blockDim.x;
@@ -1423,38 +1502,28 @@ __global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) {
     double U[9], V[9], sg[3];
     svd3_warm(Ft, U, sg, V);
     double hfin[3];
-    float Fout[9];
-    bool changed = false;
+    bool changed = false, queued = false;
     if (P.plastic_model != PL_NONE) {
       ReturnMapOut rm;
-      return_map(P, dt, sg, epd, epv, epp, dgam, plastic, err, rm);
+      return_map(P, B, (uint32_t)i, dt, sg, U, V, epd, epv, epp, dgam, plastic, niters, nsolves, err, rm);
       changed = rm.changed;
+      queued = rm.queued;
       if (rm.to_rotation) { hfin[0] = hfin[1] = hfin[2] = 0.0; }
       else for (int k = 0; k < 3; ++k) hfin[k] = rm.h[k];
     }
-    if (changed) {
-      double e[3] = {exp(hfin[0]), exp(hfin[1]), exp(hfin[2])};
+    if (!changed) for (int k = 0; k < 3; ++k) hfin[k] = log(fabs(sg[k]));
+    if (!queued) {  // queued particles get F, tau, eps_pl_dev and delta_gamma from the surrogate pass
+      float Fout[9], tau[6];
+      finish_F_tau(P, U, V, hfin, changed, Ft, Fout, tau);
 #pragma unroll
-      for (int r = 0; r < 3; ++r)
+      for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = Fout[k];
 #pragma unroll
-        for (int q = 0; q < 3; ++q)
-          Fout[3 * r + q] = (float)(U[3 * r] * e[0] * V[3 * q] + U[3 * r + 1] * e[1] * V[3 * q + 1] + U[3 * r + 2] * e[2] * V[3 * q + 2]);
-    } else {
-      for (int k = 0; k < 3; ++k) hfin[k] = log(fabs(sg[k]));
-#pragma unroll
-      for (int k = 0; k < 9; ++k) Fout[k] = (float)Ft[k];
+      for (int k = 0; k < 6; ++k) po[(F_TAU + k) * S + i] = tau[k];
+      po[F_EPD * S + i] = epd;
+      po[F_DG * S + i] = dgam;
     }
-    // Kirchhoff stress of the final F: tau = U diag(2 mu h + lambda tr h) U^T (simulation.hpp:287-294)
-    float tau[6];
-    {
-      const double tr = hfin[0] + hfin[1] + hfin[2];
-      double d[3];
-      for (int k = 0; k < 3; ++k) d[k] = 2.0 * P.mu * hfin[k] + P.lambda * tr;
-      if (!(isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2]))) { d[0] = d[1] = d[2] = 0.0; }
-      auto T = [&](int r, int q) { return U[3 * r] * d[0] * U[3 * q] + U[3 * r + 1] * d[1] * U[3 * q + 1] + U[3 * r + 2] * d[2] * U[3 * q + 2]; };
-      tau[0] = (float)T(0, 0); tau[1] = (float)T(1, 1); tau[2] = (float)T(2, 2);
-      tau[3] = (float)T(0, 1); tau[4] = (float)T(0, 2); tau[5] = (float)T(1, 2);
-    }
+    po[F_EPV * S + i] = epv;
+    po[F_EPP * S + i] = epp;
     // position update (position_update.cpp:6-91)
     float pic[3], v[3];
 #pragma unroll
@@ -1490,11 +1559,6 @@ __global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) {
     }
 #pragma unroll
     for (int r = 0; r < 3; ++r) { po[(F_X + r) * S + i] = xn[r]; po[(F_V + r) * S + i] = v[r]; }
-#pragma unroll
-    for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = Fout[k];
-    po[F_EPD * S + i] = epd; po[F_EPV * S + i] = epv; po[F_EPP * S + i] = epp; po[F_DG * S + i] = dgam;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) po[(F_TAU + k) * S + i] = tau[k];
     B.meta_out[i] = active ? meta : (meta | kInactiveBit);
     if (active) {
       ++nact;
@@ -1510,9 +1574,12 @@ __global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) {
   uint32_t na = __reduce_add_sync(0xffffffffu, nact);
   uint32_t pc = __reduce_add_sync(0xffffffffu, plastic);
   uint32_t er = __reduce_or_sync(0xffffffffu, err);
+  const uint32_t ni = __reduce_add_sync(0xffffffffu, niters), ns = __reduce_add_sync(0xffffffffu, nsolves);
   int r6[6];
   for (int r = 0; r < 3; ++r) { r6[r] = __reduce_min_sync(0xffffffffu, mn[r]); r6[3 + r] = __reduce_max_sync(0xffffffffu, mx[r]); }
   if (lane == 0) {
+    if (ni) atomicAdd(&B.ctrl->newton_iters, ni);
+    if (ns) atomicAdd(&B.ctrl->newton_solves, ns);
     red_u[warp][0] = mv; red_u[warp][1] = na; red_u[warp][2] = pc; red_u[warp][3] = er;
     for (int k = 0; k < 6; ++k) red_i[warp][k] = r6[k];
   }
@@ -1533,6 +1600,59 @@ __global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) {
     }
     if (red_u[0][2]) atomicAdd(&cw->plastic_count, red_u[0][2]);
     if (red_u[0][3]) atomicOr(&cw->error_flags, red_u[0][3]);
+  }
+}
+
+// Surrogate pass: each queued particle turns the network's plastic strain into an estimate of
+// the consistency parameter along its flow direction and checks it against the Perzyna
+// consistency condition (|r| < 1e-2 Pa, the reference's Newton tolerance).  Estimates that fail
+// drop to the plain Newton solve -- continued from the estimate, or restarted from the
+// reference's initial guess when sur_fallback_plain is set.  The final F, stress, eps_pl_dev and
+// delta_gamma are written as the plain path writes them.
+__global__ void __launch_bounds__(128) k_sur_finish(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  const uint32_t n = min(c->q_n, P.q_cap);
+  const double dt = c->dt;
+  const int S = P.np_stride;
+  uint32_t err = 0, iters = 0, accepted = 0;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const SurQ& r = B.q[k];
+    const float* y = B.qy + (size_t)k * 6;
+    double pd = 0.0, pr = 0.0;
+    for (int j = 0; j < 3; ++j) { pd += (double)y[j] * r.hd[j]; pr += (double)y[3 + j] * r.hd[j]; }
+    double dg = P.d_prefac * 0.5 * (pd + pr * dt);
+    const double dg_max = r.q_trial / P.f_mu_prefac;
+    if (!(dg >= 0.0)) dg = 0.0;
+    if (dg > dg_max) dg = dg_max;
+    uint32_t it = 0;
+    const bool vm = r.vm != 0;
+    double dgf = perzyna_newton(P, vm, r.q_trial, r.q_y, (double)r.epd, dt, dg, it, err);
+    if (it == 0) ++accepted;
+    else if (P.sur_fallback_plain) {
+      it = 0;
+      dgf = perzyna_newton(P, vm, r.q_trial, r.q_y, (double)r.epd, dt, 0.01 * (r.q_trial - r.q_y) / P.f_mu_prefac, it, err);
+    }
+    iters += it;
+    double hfin[3];
+    for (int j = 0; j < 3; ++j) hfin[j] = r.h[j] - (dgf / P.d_prefac) * r.hd[j];
+    float Fout[9], tau[6];
+    finish_F_tau(P, r.U, r.V, hfin, true, nullptr, Fout, tau);
+    float* po = B.pout;
+    const uint32_t i = r.i;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) po[(F_F + q) * S + i] = Fout[q];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) po[(F_TAU + q) * S + i] = tau[q];
+    po[F_EPD * S + i] = (float)((double)r.epd + dgf / P.d_prefac);
+    po[F_DG * S + i] = (float)(dgf / dt);
+  }
+  const uint32_t ni = __reduce_add_sync(0xffffffffu, iters), na = __reduce_add_sync(0xffffffffu, accepted);
+  const uint32_t er = __reduce_or_sync(0xffffffffu, err);
+  if ((threadIdx.x & 31) == 0) {
+    if (ni) atomicAdd(&B.ctrl->newton_iters, ni);
+    if (na) atomicAdd(&B.ctrl->sur_accept, na);
+    if (er) atomicOr(&B.ctrl->error_flags, er);
   }
 }
 
@@ -1640,6 +1760,8 @@ cudaError_t launch_init(int device) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_p2g, k_p2g, kThreads, p2g_smem_bytes());
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_g2p, k_g2p_musl, kThreads, g2p_smem_bytes());
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_def, k_defgrad, kThreads, 0);
+  e = mlp_init();
+  if (e != cudaSuccess) return e;
   if (g_occ_p2g < 1) g_occ_p2g = 1;
   if (g_occ_g2p < 1) g_occ_g2p = 1;
   if (g_occ_def < 1) g_occ_def = 1;
@@ -1648,48 +1770,42 @@ cudaError_t launch_init(int device) {
 
 int num_sms() { return g_num_sms; }
 
-void launch_step(const Params& P, const Bufs& B, cudaStream_t s) {
-  const int sms = g_num_sms > 0 ? g_num_sms : 148;
-  const int flat_grid = sms * 8;
-  k_prologue<<<1, 32, 0, s>>>(P, B);
-  k_clear<<<flat_grid, 256, 0, s>>>(P, B);
-  k_count<<<flat_grid, 256, 0, s>>>(P, B);
-  const int scan_blocks = (P.node_cap + 1 + kScanBlock - 1) / kScanBlock;
-  k_scan_local<<<scan_blocks, kScanThreads, 0, s>>>(P, B);
-  k_scan_top<<<1, kScanThreads, 0, s>>>(P, B);
-  k_scan_add<<<scan_blocks, kScanThreads, 0, s>>>(P, B);
-  k_scatter<<<flat_grid, 256, 0, s>>>(P, B);
-  k_p2g<<<sms * g_occ_p2g, kThreads, p2g_smem_bytes(), s>>>(P, B);
-  k_grid_update<<<flat_grid, 256, 0, s>>>(P, B);
-  k_g2p_musl<<<sms * g_occ_g2p, kThreads, g2p_smem_bytes(), s>>>(P, B);
-  k_defgrad<<<sms * g_occ_def, kThreads, 0, s>>>(P, B);
-  k_epilogue<<<1, 32, 0, s>>>(P, B);
+// The kernels of one step in launch order (the surrogate pass adds k_mlp_infer and k_sur_finish).
+static const char* kKernelNames[14] = {"k_prologue",    "k_clear",     "k_count",      "k_scan_local", "k_scan_top",
+                                       "k_scan_add",    "k_scatter",   "k_p2g",        "k_grid_update", "k_g2p_musl",
+                                       "k_defgrad",     "k_mlp_infer", "k_sur_finish", "k_epilogue"};
+int kernels_per_step(const Params& P) { return P.return_map == 1 ? 14 : 12; }
+const char* kernel_name(int i, const Params& P) {
+  if (i < 0 || i >= kernels_per_step(P)) return "";
+  if (P.return_map != 1 && i == 11) return kKernelNames[13];
+  return kKernelNames[i];
 }
 
-int kernels_per_step() { return 12; }
-
-static const char* kKernelNames[12] = {"k_prologue", "k_clear", "k_count", "k_scan_local", "k_scan_top", "k_scan_add",
-                                       "k_scatter", "k_p2g", "k_grid_update", "k_g2p_musl", "k_defgrad", "k_epilogue"};
-const char* kernel_name(int i) { return (i >= 0 && i < 12) ? kKernelNames[i] : ""; }
-
-// The same 12 launches with an event recorded after each (events[0] before the first).
-void launch_step_timed(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev) {
+// One step on stream s; when ev is not null an event is recorded before the first kernel and
+// after every kernel (ev must hold kernels_per_step + 1 events).
+void launch_step(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev) {
   const int sms = g_num_sms > 0 ? g_num_sms : 148;
   const int flat_grid = sms * 8;
   const int scan_blocks = (P.node_cap + 1 + kScanBlock - 1) / kScanBlock;
-  cudaEventRecord(ev[0], s);
-  k_prologue<<<1, 32, 0, s>>>(P, B); cudaEventRecord(ev[1], s);
-  k_clear<<<flat_grid, 256, 0, s>>>(P, B); cudaEventRecord(ev[2], s);
-  k_count<<<flat_grid, 256, 0, s>>>(P, B); cudaEventRecord(ev[3], s);
-  k_scan_local<<<scan_blocks, kScanThreads, 0, s>>>(P, B); cudaEventRecord(ev[4], s);
-  k_scan_top<<<1, kScanThreads, 0, s>>>(P, B); cudaEventRecord(ev[5], s);
-  k_scan_add<<<scan_blocks, kScanThreads, 0, s>>>(P, B); cudaEventRecord(ev[6], s);
-  k_scatter<<<flat_grid, 256, 0, s>>>(P, B); cudaEventRecord(ev[7], s);
-  k_p2g<<<sms * g_occ_p2g, kThreads, p2g_smem_bytes(), s>>>(P, B); cudaEventRecord(ev[8], s);
-  k_grid_update<<<flat_grid, 256, 0, s>>>(P, B); cudaEventRecord(ev[9], s);
-  k_g2p_musl<<<sms * g_occ_g2p, kThreads, g2p_smem_bytes(), s>>>(P, B); cudaEventRecord(ev[10], s);
-  k_defgrad<<<sms * g_occ_def, kThreads, 0, s>>>(P, B); cudaEventRecord(ev[11], s);
-  k_epilogue<<<1, 32, 0, s>>>(P, B); cudaEventRecord(ev[12], s);
+  int e = 0;
+  auto mark = [&]() { if (ev) cudaEventRecord(ev[e++], s); };
+  mark();
+  k_prologue<<<1, 32, 0, s>>>(P, B); mark();
+  k_clear<<<flat_grid, 256, 0, s>>>(P, B); mark();
+  k_count<<<flat_grid, 256, 0, s>>>(P, B); mark();
+  k_scan_local<<<scan_blocks, kScanThreads, 0, s>>>(P, B); mark();
+  k_scan_top<<<1, kScanThreads, 0, s>>>(P, B); mark();
+  k_scan_add<<<scan_blocks, kScanThreads, 0, s>>>(P, B); mark();
+  k_scatter<<<flat_grid, 256, 0, s>>>(P, B); mark();
+  k_p2g<<<sms * g_occ_p2g, kThreads, p2g_smem_bytes(), s>>>(P, B); mark();
+  k_grid_update<<<flat_grid, 256, 0, s>>>(P, B); mark();
+  k_g2p_musl<<<sms * g_occ_g2p, kThreads, g2p_smem_bytes(), s>>>(P, B); mark();
+  k_defgrad<<<sms * g_occ_def, kThreads, 0, s>>>(P, B); mark();
+  if (P.return_map == 1) {
+    mlp_infer(B.mlp, B.qx, B.qy, 0, &B.ctrl->q_n, (int)P.q_cap, s); mark();
+    k_sur_finish<<<sms * 8, 128, 0, s>>>(P, B); mark();
+  }
+  k_epilogue<<<1, 32, 0, s>>>(P, B); mark();
 }
 
 void launch_upload(const Params& P, const float* x, const float* lat, const float* v, float* pbuf, uint32_t* meta,

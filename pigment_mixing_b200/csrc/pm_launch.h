@@ -9,16 +9,15 @@ namespace pm {
 
 cudaError_t launch_init(int device);
 int num_sms();
-int kernels_per_step();
+int kernels_per_step(const Params& P);
+const char* kernel_name(int i, const Params& P);
 size_t p2g_smem_bytes();
 size_t g2p_smem_bytes();
-// One full step (the 12 kernels above) on stream s.
-void launch_step(const Params& P, const Bufs& B, cudaStream_t s);
+// One full step on stream s; with ev, events before and after every kernel (kernels_per_step + 1).
+void launch_step(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev = nullptr);
 void launch_reduce_state(const Params& P, const float* pcur, const uint32_t* meta, Ctrl* ctrl, cudaStream_t s);
 void launch_unpermute(const Params& P, const float* pcur, const uint32_t* meta, float* out, uint8_t* active,
                       cudaStream_t s);
-const char* kernel_name(int i);
-void launch_step_timed(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev /* 13 events */);
 void launch_upload(const Params& P, const float* x, const float* lat, const float* v, float* pbuf, uint32_t* meta,
                    cudaStream_t s);
 void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, double* acc, cudaStream_t s);

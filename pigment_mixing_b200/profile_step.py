@@ -17,11 +17,13 @@ def main():
     ap.add_argument("--warm", type=int, default=10, help="steps through advance() first")
     ap.add_argument("--profile", type=int, default=3, help="event-timed steps")
     ap.add_argument("--plain", type=int, default=3, help="plain step() calls at the end")
-    ap.add_argument("--perzyna-exp", type=float, default=None)
+    ap.add_argument("--set", action="append", default=[], metavar="NAME=VALUE",
+                    help="override a scene parameter, e.g. --set perzyna_exp=1")
     a = ap.parse_args()
     sc = WORKLOADS[a.workload]()
-    if a.perzyna_exp is not None:
-        sc["params"]["perzyna_exp"] = a.perzyna_exp
+    for kv in a.set:
+        k, v = kv.split("=", 1)
+        sc["params"][k] = float(v)
     sim = Simulation(0)
     scenes.apply(sc, sim)
     sim.prepareSimulation()

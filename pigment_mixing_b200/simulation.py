@@ -21,7 +21,7 @@ _SCALARS = ("cfl", "cfl_elastic", "flip_ratio", "rho", "E", "nu", "fps", "end_fr
             "particle_mass", "particle_volume", "plastic_model", "use_pradhana", "use_musl",
             "use_particle_boundaries", "q_max", "q_min", "p_min", "M", "q_cohesion", "perzyna_exp",
             "perzyna_visc", "xi", "q_prefac", "pigment_D_max", "pigment_D_edge0", "pigment_D_edge1",
-            "start_boost_time", "end_boost_time", "boost_factor", "auto_frame")
+            "start_boost_time", "end_boost_time", "boost_factor", "auto_frame", "surrogate_fallback_plain")
 _READONLY = ("time", "dt", "step", "Np", "mu", "lambda", "K", "dt_max", "frame_dt", "final_time",
              "n_active", "plastic_count", "grid_nodes", "frame", "kernels_per_step")
 _VECTORS = ("gravity", "particle_boundary_min", "particle_boundary_max", "grid_reference_point")
@@ -182,6 +182,29 @@ class Simulation:
     def setReturnMap(self, mode: int) -> None:
         call("pm_set_return_map", self._h, int(mode))
 
+    def setSurrogate(self, params) -> None:
+        """Load surrogate MLP weights (PM_MLP_NPARAMS floats, see pigment_mixing_b200.surrogate)."""
+        p = _f32(params).reshape(-1)
+        call("pm_set_surrogate", self._h, _fp(p))
+
+    def enableSampleLog(self, capacity: int) -> None:
+        call("pm_enable_sample_log", self._h, int(capacity))
+
+    def samples(self, max_samples: int = 1 << 26):
+        """(features[n,10], targets[n,6]) logged by the plain return map."""
+        st = self.returnMapStats()
+        m = min(int(st["logged"]), int(max_samples))
+        x = np.zeros((max(m, 1), 10), np.float32)
+        y = np.zeros((max(m, 1), 6), np.float32)
+        n = C.c_uint32()
+        call("pm_get_samples", self._h, _fp(x), _fp(y), m, C.byref(n))
+        return x[: n.value], y[: n.value]
+
+    def returnMapStats(self) -> dict:
+        a = np.zeros(5, np.uint32)
+        call("pm_get_return_map_stats", self._h, a.ctypes.data_as(C.POINTER(C.c_uint32)))
+        return dict(solves=int(a[0]), newton_iters=int(a[1]), queued=int(a[2]), accepted=int(a[3]), logged=int(a[4]))
+
     # ---- readback ------------------------------------------------------------------------------
     def getParticles(self, fields=("x", "v", "latent", "diffusion", "active")) -> Particles:
         n = self._np
@@ -215,7 +238,7 @@ class Simulation:
         k = int(self.kernels_per_step)
         ms = np.zeros(k, np.float32)
         call("pm_profile_steps", self._h, int(nsteps), _fp(ms), k)
-        return {lib().pm_kernel_name(i).decode(): float(ms[i]) for i in range(k)}
+        return {lib().pm_kernel_name(self._h, i).decode(): float(ms[i]) for i in range(k)}
 
     def errorFlags(self, clear: bool = False) -> int:
         f = C.c_uint32()
