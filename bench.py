@@ -222,6 +222,9 @@ def run_ours(args):
         _barrier(dist, device)
     clocks = clk.summary()
     flags = sim.errorFlags()
+    ref = sim.getParticles(fields=("x", "latent"))
+    x_ref, lat_ref = ref.x, ref.latent
+    newton_plain = _newton_per_solve(sim, 4)
     ms_max = _max_over_ranks(dist, ms, device)
     value = ws * npart * args.steps / (ms_max / 1e3)
     # -------- per-kernel times (CUDA events on the same stream, separate steps) --------
@@ -250,6 +253,9 @@ def run_ours(args):
     step_roof = {"bytes": step_bytes, "achieved": step_bytes / (step_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                  "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak, "active_nodes": active_nodes}
     sim.close()
+    sur = None
+    if not args.no_surrogate:
+        sur = _surrogate_leg(scene, args, device, dist, ws, value, x_ref, lat_ref, newton_plain)
     # -------- end to end through the C ABI from pinned host buffers --------
     e2e = _e2e(scene, args, device, dist, ws)
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
@@ -258,12 +264,73 @@ def run_ours(args):
             "roofline": roof, "step_roofline": step_roof, "e2e": e2e, "clocks": clocks,
             "gpu_launches": args.steps * kps,
             "kernel_ms": kms, "error_flags": flags}
+    if sur is not None:
+        line["surrogate"] = sur
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline(scene).items() if k != "seconds"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def _newton_per_solve(sim, steps):
+    it = sv = acc = 0
+    for _ in range(steps):
+        sim.advance(1)
+        st = sim.returnMapStats()
+        it += st["newton_iters"]
+        sv += st["solves"]
+        acc += st["accepted"]
+    return {"updates_per_solve": it / max(sv, 1), "solves": sv, "accepted_fraction": acc / max(sv, 1)}
+
+
+def _surrogate_leg(scene, args, device, dist, ws, plain_value, x_ref, lat_ref, newton_plain):
+    """Surrogate + FP32 form: samples logged by the plain solver on this workload, GPU training,
+    then the same warm-up + timed steps with the learned return map."""
+    import torch
+    from pigment_mixing_b200 import RETURN_MAP_SURROGATE, Simulation, scenes, surrogate
+    npart = len(scene["x"])
+    log = Simulation(device)
+    scenes.apply(scene, log)
+    every = max(1, int(round(npart * args.log_steps / 4e6)))  # about 4M samples spread over the logged steps
+    log.set(sample_log_every=every)
+    log.enableSampleLog(6 << 20)
+    log.prepareSimulation()
+    log.advance(args.log_steps)
+    xs, ys = log.samples()
+    log.close()
+    t0 = time.perf_counter()
+    params, hist = surrogate.train(xs, ys, epochs=args.train_epochs, batch=8192, lr=3e-3, seed=0)
+    train_s = time.perf_counter() - t0
+    s = Simulation(device)
+    scenes.apply(scene, s)
+    s.setSurrogate(params)
+    s.setReturnMap(RETURN_MAP_SURROGATE)
+    s.prepareSimulation()
+    s.advance(args.warmup)
+    stream = torch.cuda.ExternalStream(s.stream(), device=device)
+    _barrier(dist, device)
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.advance(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = _max_over_ranks(dist, e0.elapsed_time(e1), device)
+    value = ws * npart * args.steps / (ms / 1e3)
+    p = s.getParticles(fields=("x", "latent"))
+    dx = float(np.abs(p.x.astype(np.float64) - x_ref).max())
+    dl = float(np.abs(p.latent.astype(np.float64) - lat_ref).max())
+    newton_sur = _newton_per_solve(s, 4)
+    kms = s.profileSteps(3)
+    s.close()
+    return {"value": value, "unit": METRIC, "ms_per_step": ms / args.steps, "speedup_vs_plain": value / plain_value,
+            "train": {"samples": int(len(xs)), "logged_steps": args.log_steps, "log_every": every, "epochs": args.train_epochs,
+                      "seconds": train_s, "loss_first_epoch": float(hist[0]), "loss_last_epoch": float(hist[-1])},
+            "newton": {"plain": newton_plain, "surrogate": newton_sur},
+            "max_position_diff_vs_plain": dx, "max_latent_diff_vs_plain": dl,
+            "kernel_ms": {k: kms[k] for k in ("k_defgrad", "k_mlp_infer", "k_sur_finish") if k in kms}}
 
 
 def _e2e(scene, args, device, dist, ws):
@@ -315,8 +382,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="2m", choices=["2m", "8m", "32k"])
-    ap.add_argument("--return-map", default="plain", choices=["plain"])
+    ap.add_argument("--return-map", default="plain", choices=["plain"],
+                    help="return map of the headline value (the surrogate form is reported beside it)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the learned return-map leg")
+    ap.add_argument("--log-steps", type=int, default=20, help="plain steps logged for surrogate training")
+    ap.add_argument("--train-epochs", type=int, default=6)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -128,6 +128,7 @@ struct pm_sim {
   int sur_fallback_plain = 0;
   float* d_slog = nullptr;     // return-map sample log: log_cap x 16 floats
   uint32_t log_cap = 0;
+  uint32_t log_every = 1;
   SurQ* d_q = nullptr;         // surrogate queue (q_cap records + inputs and outputs)
   float* d_qx = nullptr;
   float* d_qy = nullptr;
@@ -305,6 +306,7 @@ void pm_sim::fill_params() {
   p.return_map = (return_map == PM_RETURN_MAP_SURROGATE && has_mlp && d_q) ? 1 : 0;
   p.sur_fallback_plain = sur_fallback_plain;
   p.log_cap = d_slog ? log_cap : 0;
+  p.log_every = log_every;
   p.q_cap = d_q ? q_cap : 0;
   graphs_dirty = true;
 }
@@ -466,7 +468,10 @@ pm_status pm_set_param(pm_sim* sim, const char* name, double v) {
   else if (k == "frame") { ctrl_field = true; }
   else if (k == "auto_frame") { h.auto_frame = v != 0; ctrl_field = true; }
   else if (k == "surrogate_fallback_plain") { sim->sur_fallback_plain = v != 0; }
-  else return fail(PM_ERR_INVALID, "unknown parameter " + k);
+  else if (k == "sample_log_every") {
+    if (!(v >= 1.0 && v <= 1e6)) return fail(PM_ERR_INVALID, "sample_log_every must be in [1, 1e6]");
+    sim->log_every = (uint32_t)v;
+  } else return fail(PM_ERR_INVALID, "unknown parameter " + k);
   if (sim->prepared) {
     if (k == "dx") return fail(PM_ERR_STATE, "dx cannot change after prepare");
     if (ctrl_field) {
@@ -502,6 +507,7 @@ pm_status pm_get_param(pm_sim* sim, const char* name, double* out) {
   else if (k == "grid_nodes") *out = c->n_nodes;
   else if (k == "kernels_per_step") *out = kernels_per_step(sim->P);
   else if (k == "surrogate_fallback_plain") *out = sim->sur_fallback_plain;
+  else if (k == "sample_log_every") *out = sim->log_every;
   else if (k == "Np") *out = sim->np;
   else if (k == "fps") *out = h.fps;
   else if (k == "cfl") *out = h.cfl;

@@ -124,6 +124,7 @@ struct Params {
   int return_map;         // 0 plain, 1 surrogate
   int sur_fallback_plain; // surrogate mode: 1 = failed checks restart Newton from the reference guess
   uint32_t log_cap;       // capacity of the return-map sample log (0 = off)
+  uint32_t log_every;     // log about one solve in log_every (hash of slot index and step)
   uint32_t q_cap;         // capacity of the surrogate queue
 };
 

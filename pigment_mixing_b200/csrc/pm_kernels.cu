@@ -1295,7 +1295,7 @@ __device__ bool newton_path(const Params& P, const Bufs& B, uint32_t i, bool vm,
     err |= E_CAPACITY;  // queue full: solve here
   }
   dg = perzyna_newton(P, vm, q_trial, q_yield, (double)epd, dt, 0.01 * (q_trial - q_yield) / P.f_mu_prefac, iters, err);
-  if (P.log_cap > 0) {
+  if (P.log_cap > 0 && (P.log_every <= 1 || ((i ^ (B.ctrl->step * 0x9E3779B9u)) * 0x85EBCA6Bu >> 8) % P.log_every == 0)) {
     const uint32_t slot = atomicAdd(&B.ctrl->slog_n, 1u);
     if (slot < P.log_cap) {
       float* o = B.slog + (size_t)slot * 16;

@@ -21,7 +21,8 @@ _SCALARS = ("cfl", "cfl_elastic", "flip_ratio", "rho", "E", "nu", "fps", "end_fr
             "particle_mass", "particle_volume", "plastic_model", "use_pradhana", "use_musl",
             "use_particle_boundaries", "q_max", "q_min", "p_min", "M", "q_cohesion", "perzyna_exp",
             "perzyna_visc", "xi", "q_prefac", "pigment_D_max", "pigment_D_edge0", "pigment_D_edge1",
-            "start_boost_time", "end_boost_time", "boost_factor", "auto_frame", "surrogate_fallback_plain")
+            "start_boost_time", "end_boost_time", "boost_factor", "auto_frame", "surrogate_fallback_plain",
+            "sample_log_every")
 _READONLY = ("time", "dt", "step", "Np", "mu", "lambda", "K", "dt_max", "frame_dt", "final_time",
              "n_active", "plastic_count", "grid_nodes", "frame", "kernels_per_step")
 _VECTORS = ("gravity", "particle_boundary_min", "particle_boundary_max", "grid_reference_point")
