@@ -39,7 +39,7 @@ ALGO_BYTES = {
     "k_g2p_musl": (144.0, 108.0),    # read x,v,latent + write v,B,latent,diff,pic ; read grid + MUSL grid
     "k_defgrad": (136.0, 12.0),      # read x,pic,F,plastic + write x,F,plastic ; read MUSL velocity
     "k_grid_update": (0.0, 40.0),    # read 16 B, write v and flip 24 B per node
-    "k_clear": (0.0, 48.0),          # zero the accumulated record
+    "k_clear_bricks": (0.0, 80.0),   # zero the accumulated and MUSL records of touched bricks
 }
 STEP_BYTES = (408.0, 256.0)          # whole step: 408 B per particle + 256 B per active node
 
@@ -170,6 +170,85 @@ def cpu_baseline(scene, budget_s: float = 25.0, max_steps: int = 20):
                       f"(CPU restatement of the reference step, float, OpenMP)", "seconds": el}
 
 
+def _err_stats(a, b):
+    d = np.linalg.norm(np.asarray(a, np.float64).reshape(len(a), -1) - np.asarray(b, np.float64).reshape(len(b), -1),
+                       axis=1)
+    return {"max": float(d.max()), "p99": float(np.percentile(d, 99))}
+
+
+def accuracy_vs_oracle(scene, steps=50, surrogate_params=None, device=0):
+    """Error of the GPU path against the FP64 oracle (the checker) on the same seeded scene after
+    ``steps`` steps: per-particle |dx| / domain size, |dv|, |d latent| (max and p99), total mass
+    and momentum, mass-weighted mean latent."""
+    from oracle.oracle import OracleSim
+    from pigment_mixing_b200 import RETURN_MAP_SURROGATE, Simulation, scenes
+    o = OracleSim(64)
+    o.set(n_threads=os.cpu_count() or 1)
+    scenes.apply(scene, o)
+    o.prepare()
+    o.advance(steps)
+    po = o.particles_f64()
+    out = {"scene": f"{scene['name']}: {len(scene['x'])} particles", "steps": steps, "domain_size": 1.0}
+    forms = [("plain", None)] + ([("surrogate", surrogate_params)] if surrogate_params is not None else [])
+    mp = scene["params"]["particle_mass"]
+    for name, params in forms:
+        g = Simulation(device)
+        scenes.apply(scene, g)
+        if params is not None:
+            g.setSurrogate(params)
+            g.setReturnMap(RETURN_MAP_SURROGATE)
+        g.prepareSimulation()
+        g.advance(steps)
+        pg = g.getParticles(fields=("x", "v", "latent"))
+        st = g.stats()
+        g.close()
+        mom_o = mp * po["v"].sum(0)
+        out[name] = {"position": _err_stats(pg.x, po["x"]), "velocity": _err_stats(pg.v, po["v"]),
+                     "latent": _err_stats(pg.latent, po["latent"]),
+                     "mass_rel": abs(st["mass"] - mp * len(scene["x"])) / (mp * len(scene["x"])),
+                     "momentum_abs": float(np.abs(st["momentum"] - mom_o).max()),
+                     "momentum_scale": float(np.abs(mom_o).max()),
+                     "mean_latent_abs": float(np.abs(st["mean_latent"] - po["latent"].mean(0)).max())}
+    return out
+
+
+def drift(scene, steps, device=0):
+    """Mass and mass-weighted mean latent of the GPU path at step 0 and after ``steps`` steps."""
+    from pigment_mixing_b200 import Simulation, scenes
+    g = Simulation(device)
+    scenes.apply(scene, g)
+    g.prepareSimulation()
+    s0 = g.stats()
+    import torch
+    stream = torch.cuda.ExternalStream(g.stream(), device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    seg = max(1, steps // 10)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range((steps + seg - 1) // seg + 1)]
+    torch.cuda.synchronize(device)
+    ev[0].record(stream)
+    done = 0
+    for j in range(1, len(ev)):
+        k = min(seg, steps - done)
+        g.advance(k)
+        done += k
+        ev[j].record(stream)
+    torch.cuda.synchronize(device)
+    ms = ev[0].elapsed_time(ev[-1])
+    seg_ms = [ev[j - 1].elapsed_time(ev[j]) / seg for j in range(1, len(ev))]
+    s1 = g.stats()
+    flags = g.errorFlags()
+    nodes = int(g.grid_nodes)
+    regrow = {"count": int(g.regrowths), "host_ms": float(g.regrow_ms),
+              "capacity_nodes_end": int(g.grid_capacity_nodes)}
+    g.close()
+    return {"steps": steps, "ms_per_step_avg": ms / steps, "ms_per_step_by_segment": seg_ms,
+            "particle_steps_per_s": len(scene["x"]) * steps / (ms / 1e3),
+            "mass_rel": abs(s1["mass"] - s0["mass"]) / s0["mass"],
+            "mean_latent_abs": float(np.abs(s1["mean_latent"] - s0["mean_latent"]).max()),
+            "momentum_step_end": [float(v) for v in s1["momentum"]], "n_active_end": int(s1["n_active"]),
+            "grid_nodes_end": nodes, "grid_regrowth": regrow, "error_flags": int(flags)}
+
+
 def run_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return  # replicas: rank 0 alone times the CPU path
@@ -237,14 +316,7 @@ def run_ours(args):
     pb, nb = ALGO_BYTES[dom]
     algo = pb * npart + nb * active_nodes
     achieved = algo / (kms[dom] / 1e3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic_2m.json")
-    if args.workload == "2m" and os.path.exists(tpath):
-        try:
-            with open(tpath) as f:
-                traffic = json.load(f).get(dom)
-        except Exception:
-            traffic = None
+    traffic = _ncu_traffic(dom) if args.workload == "2m" else None
     step_ms = ms_max / args.steps
     step_bytes = STEP_BYTES[0] * npart + STEP_BYTES[1] * active_nodes
     roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -266,12 +338,33 @@ def run_ours(args):
             "kernel_ms": kms, "error_flags": flags}
     if sur is not None:
         line["surrogate"] = sur
+    if args.drift_steps > 0:
+        line["drift"] = drift(scene, args.drift_steps, device)
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline(scene).items() if k != "seconds"}
+        # the FP64 oracle as checker: 50-step error on the 32,768-particle scene of the same recipe
+        line["accuracy"] = accuracy_vs_oracle(_workload("32k"), 50, _small_surrogate(device), device)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def _ncu_traffic(kernel):
+    """dram__bytes_read.sum + dram__bytes_write.sum per launch of ``kernel`` from the committed ncu
+    summary of the 2M scene (line ``traffic_bytes_per_launch: name=bytes ...``)."""
+    path = os.path.join(ROOT, "profiles", "k_p2g_g2p_defgrad_2m_full.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    for kv in line.split(":", 1)[1].split():
+                        k, v = kv.split("=")
+                        if k == kernel:
+                            return float(v)
+    except OSError:
+        pass
+    return None
 
 
 def _newton_per_solve(sim, steps):
@@ -333,6 +426,20 @@ def _surrogate_leg(scene, args, device, dist, ws, plain_value, x_ref, lat_ref, n
             "kernel_ms": {k: kms[k] for k in ("k_defgrad", "k_mlp_infer", "k_sur_finish") if k in kms}}
 
 
+def _small_surrogate(device):
+    """Surrogate trained on the 32,768-particle scene's own logged samples (60 plain steps)."""
+    from pigment_mixing_b200 import Simulation, scenes, surrogate
+    log = Simulation(device)
+    scenes.apply(_workload("32k"), log)
+    log.enableSampleLog(1 << 22)
+    log.prepareSimulation()
+    log.advance(60)
+    xs, ys = log.samples()
+    log.close()
+    params, _ = surrogate.train(xs, ys, epochs=20, batch=4096, lr=3e-3, seed=0)
+    return params
+
+
 def _e2e(scene, args, device, dist, ws):
     import torch
     from pigment_mixing_b200 import Simulation, scenes
@@ -387,7 +494,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned return-map leg")
     ap.add_argument("--log-steps", type=int, default=20, help="plain steps logged for surrogate training")
-    ap.add_argument("--train-epochs", type=int, default=6)
+    ap.add_argument("--train-epochs", type=int, default=30)
+    ap.add_argument("--drift-steps", type=int, default=1000,
+                    help="steps of the mass / mean-latent drift run on the workload (0 = skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cctype>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -111,10 +112,13 @@ struct pm_sim {
   uint32_t *d_key = nullptr, *d_rank = nullptr, *d_sorted = nullptr;
 
   int brick_cap = 0;
+  uint32_t regrowths = 0;   // grid reallocations so far
+  double regrow_ms = 0.0;   // host time spent in them
   uint32_t* d_cell = nullptr;
   uint32_t* d_scan_part = nullptr;
   float4* d_grid = nullptr;
   float4* d_gmusl = nullptr;
+  uint8_t* d_btouch = nullptr;
 
   Ctrl* d_ctrl = nullptr;
   Ctrl* h_ctrl = nullptr;  // pinned mirror
@@ -200,7 +204,8 @@ void pm_sim::free_grid() {
   if (d_scan_part) cudaFree(d_scan_part);
   if (d_grid) cudaFree(d_grid);
   if (d_gmusl) cudaFree(d_gmusl);
-  d_cell = nullptr; d_scan_part = nullptr; d_grid = nullptr; d_gmusl = nullptr;
+  if (d_btouch) cudaFree(d_btouch);
+  d_cell = nullptr; d_scan_part = nullptr; d_grid = nullptr; d_gmusl = nullptr; d_btouch = nullptr;
   brick_cap = 0;
 }
 
@@ -229,8 +234,10 @@ pm_status pm_sim::alloc_grid(int bricks) {
   CK(cudaMalloc(&d_scan_part, scan_blocks * sizeof(uint32_t)));
   CK(cudaMalloc(&d_grid, nodes * 4 * sizeof(float4)));
   CK(cudaMalloc(&d_gmusl, nodes * sizeof(float4)));
-  CK(cudaMemsetAsync(d_grid, 0, nodes * 4 * sizeof(float4), stream));
-  CK(cudaMemsetAsync(d_gmusl, 0, nodes * sizeof(float4), stream));
+  // grid records need no zeroing here: each step zeroes the bricks it touches (k_clear_bricks)
+  // and readers see only touched bricks
+  CK(cudaMalloc(&d_btouch, (size_t)bricks));
+  CK(cudaMemsetAsync(d_btouch, 0, (size_t)bricks, stream));
   brick_cap = bricks;
   return PM_OK;
 }
@@ -249,6 +256,7 @@ Bufs pm_sim::bufs(int parity) const {
   b.scan_part = d_scan_part;
   b.grid = d_grid;
   b.gmusl = d_gmusl;
+  b.btouch = d_btouch;
   b.ctrl = d_ctrl;
   b.mlp = mlp_dev;
   b.slog = d_slog;
@@ -339,20 +347,27 @@ pm_status pm_sim::capture_graphs() {
   return PM_OK;
 }
 
-// Runs n steps; recovers from grid-capacity halts by regrowing and resuming.
+// Runs n steps in chunks of at most kChunkSteps, reading the control block after each chunk.
+// The grid box is recomputed on the device every step; when a chunk ends with the box above
+// kGrowAt of the capacity, the grid is regrown before the next chunk (and always after a
+// capacity halt, which the device raises instead of writing out of bounds), so a halt wastes at
+// most one chunk of no-op launches.
 pm_status pm_sim::run_steps(uint32_t n, bool use_graph) {
+  constexpr uint32_t kChunkSteps = 64;
+  constexpr double kGrowAt = 0.8;
   uint32_t remaining = n;
   int guard = 0;
   while (remaining > 0) {
     const uint32_t before = host_step;
+    const uint32_t chunk = std::min(remaining, kChunkSteps);
     uint32_t k = 0;
-    if (use_graph && remaining >= 2) {
+    if (use_graph && chunk >= 2) {
       if (graphs_dirty) { pm_status s = capture_graphs(); if (s != PM_OK) return s; }
       int par = cur;
-      for (; k + 2 <= remaining; k += 2) CK(cudaGraphLaunch(gexec[par], stream));
+      for (; k + 2 <= chunk; k += 2) CK(cudaGraphLaunch(gexec[par], stream));
     }
     int par = (cur + (int)k) & 1;
-    for (; k < remaining; ++k) { launch_step(P, bufs(par), stream, nullptr); par ^= 1; }
+    for (; k < chunk; ++k) { launch_step(P, bufs(par), stream, nullptr); par ^= 1; }
     CK(cudaGetLastError());
     pm_status s = sync_ctrl();
     if (s != PM_OK) return s;
@@ -360,13 +375,21 @@ pm_status pm_sim::run_steps(uint32_t n, bool use_graph) {
     host_step = h_ctrl->step;
     cur = (cur + (int)done) & 1;
     remaining -= std::min(done, remaining);
+    if (done > 0) guard = 0;  // count only regrowths that made no progress
+    long long want = 0;
     if (h_ctrl->halt) {
       if (++guard > 8) return fail(PM_ERR_CAPACITY, "grid keeps overflowing after regrowth");
-      const int need = (int)h_ctrl->need_bricks;
-      const long long want = (long long)need * 3 / 2 + 64;
+      want = (long long)h_ctrl->need_bricks * 2 + 64;
+    } else if (remaining > 0 && h_ctrl->n_bricks > kGrowAt * brick_cap) {
+      want = (long long)h_ctrl->n_bricks * 2 + 64;
+    }
+    if (want > 0) {
       if (want * kBrickNodes > 0x7ffffff0LL) return fail(PM_ERR_CAPACITY, "grid would exceed 2^31 nodes");
+      const auto t0 = std::chrono::steady_clock::now();
       s = alloc_grid((int)want);
       if (s != PM_OK) return s;
+      ++regrowths;
+      regrow_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
       fill_params();
       h_ctrl->halt = 0;
       h_ctrl->error_flags &= ~(uint32_t)E_CAPACITY;
@@ -506,6 +529,9 @@ pm_status pm_get_param(pm_sim* sim, const char* name, double* out) {
   else if (k == "plastic_count") *out = c->plastic_count;
   else if (k == "grid_nodes") *out = c->n_nodes;
   else if (k == "kernels_per_step") *out = kernels_per_step(sim->P);
+  else if (k == "regrowths") *out = sim->regrowths;
+  else if (k == "regrow_ms") *out = sim->regrow_ms;
+  else if (k == "grid_capacity_nodes") *out = (double)sim->brick_cap * kBrickNodes;
   else if (k == "surrogate_fallback_plain") *out = sim->sur_fallback_plain;
   else if (k == "sample_log_every") *out = sim->log_every;
   else if (k == "Np") *out = sim->np;
@@ -1048,9 +1074,18 @@ pm_status pm_get_grid(pm_sim* sim, double origin[3], uint32_t dims[3], float* ma
   if (!mass && !v_update && !v_musl && !flip && !latent && !shear) return PM_OK;
   const size_t nn = (size_t)c->n_nodes;
   std::vector<float4> g(nn * 4), m(nn);
+  std::vector<uint8_t> touched(nn / kBrickNodes);
   CK(cudaMemcpyAsync(g.data(), sim->d_grid, nn * 4 * sizeof(float4), cudaMemcpyDeviceToHost, sim->stream));
   CK(cudaMemcpyAsync(m.data(), sim->d_gmusl, nn * sizeof(float4), cudaMemcpyDeviceToHost, sim->stream));
+  CK(cudaMemcpyAsync(touched.data(), sim->d_btouch, touched.size(), cudaMemcpyDeviceToHost, sim->stream));
   CK(cudaStreamSynchronize(sim->stream));
+  // bricks that no particle stencil reached this step hold stale records: report them empty
+  for (size_t b = 0; b < touched.size(); ++b)
+    if (!touched[b])
+      for (size_t n = b * kBrickNodes; n < (b + 1) * kBrickNodes; ++n) {
+        for (int q = 0; q < 4; ++q) g[n * 4 + q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        m[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
   for (int i = 0; i < c->dims[0]; ++i)
     for (int j = 0; j < c->dims[1]; ++j)
       for (int k = 0; k < c->dims[2]; ++k) {

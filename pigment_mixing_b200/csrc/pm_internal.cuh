@@ -187,6 +187,7 @@ struct Bufs {
   uint32_t* scan_part;    // per scan block partial sums
   float4* grid;           // node_cap * 4 float4
   float4* gmusl;          // node_cap float4
+  uint8_t* btouch;        // brick_cap: 1 when a particle's stencil reaches the brick this step
   Ctrl* ctrl;
   // learned return map (optional)
   MlpDev mlp;

@@ -284,14 +284,58 @@ __global__ void k_epilogue(Params P, Bufs B) {
 // ------------------------------------------------------------------------------------------
 // counting sort by cell
 // ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void brick_coords(int b, const Ctrl* c, int& bx, int& by, int& bz) {
+  const int nyz = c->nb[1] * c->nb[2];
+  bx = b / nyz;
+  int r = b - bx * nyz;
+  by = r / c->nb[2];
+  bz = r - by * c->nb[2];
+}
+
+// Zeroes the per-node counters of the counting sort (the grid records are cleared per brick by
+// k_clear_bricks once the occupied bricks are known).
 __global__ void k_clear(Params P, Bufs B) {
   const Ctrl* c = B.ctrl;
   if (c->halt) return;
   const int nn = c->n_nodes;
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn + 2; i += stride) B.cell[i] = 0u;
+}
+
+// After the scan: a brick is touched this step when one of the bricks b - d, d in {0,1}^3, holds
+// particles (a particle's 3x3x3 stencil spans its own brick and the next one on each axis).
+// One warp per brick: lanes 0..7 test the eight source bricks, then the warp zeroes the brick's
+// 64 accumulated records and MUSL records and stores the flag that k_grid_update reads.  Only
+// touched bricks are ever read by the transfers, so untouched ones are left as they are.
+__global__ void k_clear_bricks(Params P, Bufs B) {
+  const Ctrl* c = B.ctrl;
+  if (c->halt) return;
+  const int nbr = c->n_bricks, lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
   const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn * 4; i += stride) B.grid[i] = z;
+  for (int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); b < nbr; b += warps) {
+    bool occ = false;
+    if (lane < 8) {
+      int bx, by, bz;
+      brick_coords(b, c, bx, by, bz);
+      const int sx = bx - (lane >> 2), sy = by - ((lane >> 1) & 1), sz = bz - (lane & 1);
+      if (sx >= 0 && sy >= 0 && sz >= 0) {
+        const size_t sb = ((size_t)sx * c->nb[1] + sy) * c->nb[2] + sz;
+        occ = B.cell[sb * kBrickNodes] != B.cell[(sb + 1) * kBrickNodes];
+      }
+    }
+    const bool touched = __ballot_sync(0xffffffffu, occ) != 0u;
+    if (lane == 0) B.btouch[b] = touched ? 1 : 0;
+    if (!touched) continue;
+    float4* rec = B.grid + (size_t)b * kBrickNodes * 4;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) rec[k * 32 + lane] = z;
+    if (P.use_musl) {
+      float4* m = B.gmusl + (size_t)b * kBrickNodes;
+      m[lane] = z;
+      m[32 + lane] = z;
+    }
+  }
 }
 
 __device__ __forceinline__ uint32_t brick_key(const int c[3], const Ctrl* ctrl) {
@@ -456,13 +500,6 @@ static_assert(sizeof(StageP2G) == 48 * 4, "stage size");
 
 size_t p2g_smem_bytes() { return sizeof(float) * kP2GCh * kTileNodes + sizeof(StageP2G) * kThreads; }
 
-__device__ __forceinline__ void brick_coords(int b, const Ctrl* c, int& bx, int& by, int& bz) {
-  const int nyz = c->nb[1] * c->nb[2];
-  bx = b / nyz;
-  int r = b - bx * nyz;
-  by = r / c->nb[2];
-  bz = r - by * c->nb[2];
-}
 
 __device__ __forceinline__ int tile_to_node(int tn, int bx, int by, int bz, const Ctrl* c) {
   int tx = tn / 36, ty = (tn / 6) % 6, tz = tn % 6;
@@ -797,9 +834,8 @@ __global__ void k_grid_update(Params P, Bufs B) {
   const float dtg[3] = {dtf * P.gravity[0], dtf * P.gravity[1], dtf * P.gravity[2]};
   const int stride = gridDim.x * blockDim.x;
   uint32_t err = 0;
-  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += stride) {
-    if (P.use_musl) B.gmusl[n] = z;
+    if (!B.btouch[n >> 6]) continue;  // no particle stencil reaches this brick: record is stale
     float4* rec = B.grid + (size_t)n * 4;
     float4 r0 = rec[0];
     if (!(r0.x > 0.f)) continue;
@@ -1771,13 +1807,13 @@ cudaError_t launch_init(int device) {
 int num_sms() { return g_num_sms; }
 
 // The kernels of one step in launch order (the surrogate pass adds k_mlp_infer and k_sur_finish).
-static const char* kKernelNames[14] = {"k_prologue",    "k_clear",     "k_count",      "k_scan_local", "k_scan_top",
-                                       "k_scan_add",    "k_scatter",   "k_p2g",        "k_grid_update", "k_g2p_musl",
-                                       "k_defgrad",     "k_mlp_infer", "k_sur_finish", "k_epilogue"};
-int kernels_per_step(const Params& P) { return P.return_map == 1 ? 14 : 12; }
+static const char* kKernelNames[15] = {"k_prologue",    "k_clear",       "k_count",    "k_scan_local", "k_scan_top",
+                                       "k_scan_add",    "k_scatter",     "k_clear_bricks", "k_p2g",    "k_grid_update",
+                                       "k_g2p_musl",    "k_defgrad",     "k_mlp_infer", "k_sur_finish", "k_epilogue"};
+int kernels_per_step(const Params& P) { return P.return_map == 1 ? 15 : 13; }
 const char* kernel_name(int i, const Params& P) {
   if (i < 0 || i >= kernels_per_step(P)) return "";
-  if (P.return_map != 1 && i == 11) return kKernelNames[13];
+  if (P.return_map != 1 && i == 12) return kKernelNames[14];
   return kKernelNames[i];
 }
 
@@ -1797,6 +1833,7 @@ void launch_step(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev
   k_scan_top<<<1, kScanThreads, 0, s>>>(P, B); mark();
   k_scan_add<<<scan_blocks, kScanThreads, 0, s>>>(P, B); mark();
   k_scatter<<<flat_grid, 256, 0, s>>>(P, B); mark();
+  k_clear_bricks<<<flat_grid, 256, 0, s>>>(P, B); mark();
   k_p2g<<<sms * g_occ_p2g, kThreads, p2g_smem_bytes(), s>>>(P, B); mark();
   k_grid_update<<<flat_grid, 256, 0, s>>>(P, B); mark();
   k_g2p_musl<<<sms * g_occ_g2p, kThreads, g2p_smem_bytes(), s>>>(P, B); mark();

@@ -31,6 +31,14 @@ __device__ __forceinline__ float gelu(float x) {  // tanh form of GELU
   const float k0 = 0.7978845608028654f, k1 = 0.044715f;
   return 0.5f * x * (1.f + tanhf(k0 * (x + k1 * x * x * x)));
 }
+// Inference form: the SFU's tanh.approx.f32 (activations are rounded to bf16 right after).
+__device__ __forceinline__ float gelu_fast(float x) {
+  const float k0 = 0.7978845608028654f, k1 = 0.044715f;
+  const float u = k0 * (x + k1 * x * x * x);
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+  return 0.5f * x * (1.f + t);
+}
 __device__ __forceinline__ float gelu_grad(float x) {
   const float k0 = 0.7978845608028654f, k1 = 0.044715f;
   const float u = k0 * (x + k1 * x * x * x);
@@ -146,9 +154,14 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   return *reinterpret_cast<uint32_t*>(&v);
 }
 
+// Shared-memory row strides of the staged weights (bf16 elements).  Rows are padded so that the
+// eight rows a B-fragment load touches (lane group g) fall in distinct banks: 24 and 72 elements
+// are 12 and 36 words, i.e. 12 g and 4 g (mod 32) for g = 0..7.
+constexpr int kW1Ld = 24, kW2Ld = 72, kW3Ld = 72;
+
 // Warp-level forward pass of 16 samples (rows of xs[16][16], bf16, normalised, zero padded)
 // producing ys[16][8] (FP32, normalised outputs in columns 0..5).  Weights in shared memory:
-// W1s[64][16], W2s[64][64], W3s[8][64] bf16 (row n = output, k contiguous), biases FP32.
+// W1s[64][kW1Ld], W2s[64][kW2Ld], W3s[8][kW3Ld] bf16 (row n = output, k contiguous), biases FP32.
 __device__ void mlp_warp16(const MlpDev& w, const __nv_bfloat16* xs, float* ys) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   // layer 1 A fragment from xs (row-major 16 x 16)
@@ -164,13 +177,13 @@ __device__ void mlp_warp16(const MlpDev& w, const __nv_bfloat16* xs, float* ys) 
 #pragma unroll
   for (int nt = 0; nt < 8; ++nt) {
     const int n = nt * 8 + g;
-    const uint32_t* wr = reinterpret_cast<const uint32_t*>(w.W1 + n * 16);
+    const uint32_t* wr = reinterpret_cast<const uint32_t*>(w.W1 + n * kW1Ld);
     const uint32_t b[2] = {wr[t], wr[4 + t]};
     const float bias0 = w.b1[nt * 8 + 2 * t], bias1 = w.b1[nt * 8 + 2 * t + 1];
     h1[nt][0] = bias0; h1[nt][1] = bias1; h1[nt][2] = bias0; h1[nt][3] = bias1;
     mma_bf16(h1[nt], a, b);
 #pragma unroll
-    for (int r = 0; r < 4; ++r) h1[nt][r] = gelu(h1[nt][r]);
+    for (int r = 0; r < 4; ++r) h1[nt][r] = gelu_fast(h1[nt][r]);
   }
   // layer 2: A fragments of k-step j from h1 tiles 2j and 2j+1
   float h2[8][4];
@@ -185,7 +198,7 @@ __device__ void mlp_warp16(const MlpDev& w, const __nv_bfloat16* xs, float* ys) 
                             pack_bf16(h1[2 * j + 1][0], h1[2 * j + 1][1]), pack_bf16(h1[2 * j + 1][2], h1[2 * j + 1][3])};
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
-      const uint32_t* wr = reinterpret_cast<const uint32_t*>(w.W2 + (nt * 8 + g) * 64 + 16 * j);
+      const uint32_t* wr = reinterpret_cast<const uint32_t*>(w.W2 + (nt * 8 + g) * kW2Ld + 16 * j);
       const uint32_t b[2] = {wr[t], wr[4 + t]};
       mma_bf16(h2[nt], aj, b);
     }
@@ -193,7 +206,7 @@ __device__ void mlp_warp16(const MlpDev& w, const __nv_bfloat16* xs, float* ys) 
 #pragma unroll
   for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
-    for (int r = 0; r < 4; ++r) h2[nt][r] = gelu(h2[nt][r]);
+    for (int r = 0; r < 4; ++r) h2[nt][r] = gelu_fast(h2[nt][r]);
   // layer 3 (outputs padded to 8)
   float y[4];
   {
@@ -204,7 +217,7 @@ __device__ void mlp_warp16(const MlpDev& w, const __nv_bfloat16* xs, float* ys) 
   for (int j = 0; j < 4; ++j) {
     const uint32_t aj[4] = {pack_bf16(h2[2 * j][0], h2[2 * j][1]), pack_bf16(h2[2 * j][2], h2[2 * j][3]),
                             pack_bf16(h2[2 * j + 1][0], h2[2 * j + 1][1]), pack_bf16(h2[2 * j + 1][2], h2[2 * j + 1][3])};
-    const uint32_t* wr = reinterpret_cast<const uint32_t*>(w.W3 + g * 64 + 16 * j);
+    const uint32_t* wr = reinterpret_cast<const uint32_t*>(w.W3 + g * kW3Ld + 16 * j);
     const uint32_t b[2] = {wr[t], wr[4 + t]};
     mma_bf16(y, aj, b);
   }
@@ -218,12 +231,12 @@ __device__ void mlp_warp16(const MlpDev& w, const __nv_bfloat16* xs, float* ys) 
 __device__ MlpDev mlp_stage(const MlpDev& gw, unsigned char* smem) {
   MlpDev w;
   __nv_bfloat16* W1 = reinterpret_cast<__nv_bfloat16*>(smem);
-  __nv_bfloat16* W2 = W1 + 64 * 16;
-  __nv_bfloat16* W3 = W2 + 64 * 64;
-  float* f = reinterpret_cast<float*>(W3 + 8 * 64);
-  for (int i = threadIdx.x; i < 64 * 16; i += blockDim.x) W1[i] = gw.W1[i];
-  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) W2[i] = gw.W2[i];
-  for (int i = threadIdx.x; i < 8 * 64; i += blockDim.x) W3[i] = gw.W3[i];
+  __nv_bfloat16* W2 = W1 + 64 * kW1Ld;
+  __nv_bfloat16* W3 = W2 + 64 * kW2Ld;
+  float* f = reinterpret_cast<float*>(W3 + 8 * kW3Ld);
+  for (int i = threadIdx.x; i < 64 * 16; i += blockDim.x) W1[(i >> 4) * kW1Ld + (i & 15)] = gw.W1[i];
+  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) W2[(i >> 6) * kW2Ld + (i & 63)] = gw.W2[i];
+  for (int i = threadIdx.x; i < 8 * 64; i += blockDim.x) W3[(i >> 6) * kW3Ld + (i & 63)] = gw.W3[i];
   float* b1 = f;
   float* b2 = b1 + 64;
   float* b3 = b2 + 64;
@@ -241,7 +254,7 @@ __device__ MlpDev mlp_stage(const MlpDev& gw, unsigned char* smem) {
 constexpr int kMlpThreads = 128;
 constexpr int kMlpWarps = kMlpThreads / 32;
 __host__ __device__ constexpr size_t mlp_weights_smem() {
-  return (((64 * 16 + 64 * 64 + 8 * 64) * 2 + (64 + 64 + 8 + 32) * 4) + 15) / 16 * 16;
+  return (((64 * kW1Ld + 64 * kW2Ld + 8 * kW3Ld) * 2 + (64 + 64 + 8 + 32) * 4) + 15) / 16 * 16;
 }
 size_t mlp_stage_bytes() { return mlp_weights_smem(); }
 size_t mlp_infer_smem_bytes() { return mlp_weights_smem() + kMlpWarps * (256 * 2 + 128 * 4); }
@@ -263,7 +276,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_infer(MlpDev gw, const floa
     for (int e = lane; e < 256; e += 32) {
       const int r = e >> 4, k = e & 15;
       float v = 0.f;
-      if (k < 10 && r0 + r < n) v = (X[(size_t)(r0 + r) * 10 + k] - mean[k]) / sd[k];
+      if (k < 10 && r0 + r < n) v = __fdividef(X[(size_t)(r0 + r) * 10 + k] - mean[k], sd[k]);
       xs[e] = __float2bfloat16_rn(v);
     }
     __syncwarp();

@@ -79,7 +79,7 @@ def two_block_scene(dx: float, block_cells=(16, 16, 8), seed: int = 0, steps: in
                       M=float(np.tan(np.deg2rad(5.0))), q_cohesion=500.0, perzyna_exp=1.0, perzyna_visc=0.4,
                       use_pradhana=1)
     vectors = dict(gravity=[0.0, -9.81, 0.0], grid_reference_point=[0.0, 0.0, 0.0],
-                   particle_boundary_min=[-2.0, -2.0, -2.0], particle_boundary_max=[2.0, 2.0, 2.0])
+                   particle_boundary_min=[0.0, 0.0, 0.0], particle_boundary_max=[1.0, 1.0, 1.0])
     objects = [("plate", dict(pos=0.0, plate_type=1, bc=1, friction=1.0))]
     if knife:
         half = [0.2, 0.1, 0.005]
