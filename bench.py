@@ -328,6 +328,9 @@ def run_ours(args):
     sur = None
     if not args.no_surrogate:
         sur = _surrogate_leg(scene, args, device, dist, ws, value, x_ref, lat_ref, newton_plain)
+    batch = None
+    if not args.no_batch:
+        batch = _batch_leg(args, device, dist, ws)
     # -------- end to end through the C ABI from pinned host buffers --------
     e2e = _e2e(scene, args, device, dist, ws)
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
@@ -338,6 +341,8 @@ def run_ours(args):
             "kernel_ms": kms, "error_flags": flags}
     if sur is not None:
         line["surrogate"] = sur
+    if batch is not None:
+        line["batch"] = batch
     if args.drift_steps > 0:
         line["drift"] = drift(scene, args.drift_steps, device)
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -440,6 +445,72 @@ def _small_surrogate(device):
     return params
 
 
+def _batch_leg(args, device, dist, ws):
+    """The batched workload: args.batch_scenes independent palette scenes (particle counts
+    log-uniform 20k-400k, grids 64^3-160^3, random pigment pair, yield and knife path) stepped
+    together through pm_batch (autotuned launch shapes, one CUDA graph per round), against the
+    same scenes advanced one after another through the single-scene API."""
+    import torch
+    from pigment_mixing_b200 import Batch, Simulation, scenes
+    scs = scenes.batch_scenes(args.batch_scenes, seed=0)
+    npart = sum(len(sc["x"]) for sc in scs)
+
+    def make():
+        out = []
+        for sc in scs:
+            g = Simulation(device)
+            scenes.apply(sc, g)
+            g.prepareSimulation()
+            out.append(g)
+        return out
+
+    sims = make()
+    b = Batch(sims)
+    t0 = time.perf_counter()
+    tuning, tuned_ms = b.autotune(trial_rounds=3)
+    tune_s = time.perf_counter() - t0
+    b.step(args.warmup)
+    stream = torch.cuda.ExternalStream(b.stream(), device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    _barrier(dist, device)
+    torch.cuda.synchronize(device)
+    e0.record(stream)
+    b.step(args.batch_steps)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = _max_over_ranks(dist, e0.elapsed_time(e1), device)
+    value = ws * npart * args.batch_steps / (ms / 1e3)
+    prof = b.profile(3)
+    steps = sorted({g.steps_done for g in sims})
+    flags = int(np.bitwise_or.reduce([g.errorFlags() for g in sims]))
+    b.close()
+    for g in sims:
+        g.close()
+    # the same scenes, one after another through pm_advance (each synchronises at its end)
+    seq = make()
+    for g in seq:
+        g.advance(args.warmup)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for g in seq:
+        g.advance(args.batch_steps)
+    torch.cuda.synchronize(device)
+    seq_s = time.perf_counter() - t0
+    for g in seq:
+        g.close()
+    seq_value = ws * npart * args.batch_steps / seq_s
+    counts = [len(sc["x"]) for sc in scs]
+    grids = [int(round(1.0 / sc["params"]["dx"])) for sc in scs]
+    return {"value": value, "unit": METRIC, "scenes": len(scs), "particles": npart,
+            "particles_min_max": [min(counts), max(counts)], "grid_min_max": [min(grids), max(grids)],
+            "rounds": args.batch_steps, "ms_per_round": ms / args.batch_steps, "tuning": tuning,
+            "autotune_ms_per_round": tuned_ms, "autotune_seconds": tune_s,
+            "sequential_value": seq_value, "speedup_vs_sequential": value / seq_value,
+            "steps_after": steps, "error_flags": flags, "kernel_ms": prof,
+            "workload": "palette scenes: 2 blocks each, random pigment pair of 6 RGB seeds, yield U(50,200) Pa, "
+                        "random 3-segment knife path, VMVisc, MUSL, APIC, plain return map"}
+
+
 def _e2e(scene, args, device, dist, ws):
     import torch
     from pigment_mixing_b200 import Simulation, scenes
@@ -495,6 +566,9 @@ def main():
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned return-map leg")
     ap.add_argument("--log-steps", type=int, default=20, help="plain steps logged for surrogate training")
     ap.add_argument("--train-epochs", type=int, default=30)
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenes leg")
+    ap.add_argument("--batch-scenes", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=50, help="timed rounds of the batched leg")
     ap.add_argument("--drift-steps", type=int, default=1000,
                     help="steps of the mass / mean-latent drift run on the workload (0 = skip)")
     args = ap.parse_args()

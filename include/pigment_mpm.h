@@ -207,6 +207,51 @@ PM_API const char* pm_kernel_name(pm_sim* sim, int index);
  * step (pm_get_param "kernels_per_step"). */
 PM_API pm_status pm_profile_steps(pm_sim* sim, uint32_t nsteps, float* kernel_ms, uint32_t n_kernels);
 
+/* ---- batched scenes --------------------------------------------------------------------------
+ * No counterpart in the reference, which runs one Simulation per process
+ * (R/src/mpm/MPMIntegrationSim.cpp:16-38 creates one).  A batch steps many independent, prepared
+ * simulations on one GPU together: every kernel of the step is launched once for all scenes,
+ * its CTAs statically partitioned across the scenes in proportion to their work and looping over
+ * their scene's particles, bricks or nodes; one round (one step of every scene) is captured as a
+ * CUDA graph and replayed.  Scenes keep their own dt, time, frame, grid box and capacity; a scene
+ * whose grid overflows sits rounds out until the host has regrown it, so pm_batch_step(n) ends
+ * with every scene exactly n steps further.  A batch step is an advance (frame bookkeeping after
+ * every step, as pm_advance).  The batch references the simulations (it does not
+ * own them): destroy the batch first.  While a batch step runs, the member simulations must not
+ * be used on other threads; between batch steps every per-scene call works as usual. */
+typedef struct pm_batch pm_batch;
+
+/* Launch shapes of the batched kernels (what pm_batch_autotune picks). */
+typedef struct pm_batch_tuning {
+  int32_t flat_threads;      /* block size of the flat kernels: 128, 256 or 512 */
+  int32_t part_ctas_per_sm;  /* CTAs per SM, particle-parallel flat kernels (count, scatter) */
+  int32_t node_ctas_per_sm;  /* CTAs per SM, node-parallel flat kernels (clear, grid update) */
+  int32_t p2g_ctas_per_sm;   /* CTAs per SM of P2G, G2P+MUSL, deformation update, surrogate */
+  int32_t g2p_ctas_per_sm;
+  int32_t def_ctas_per_sm;
+  int32_t sur_ctas_per_sm;
+  int32_t chunk_rounds;      /* rounds replayed between host checks of the control blocks */
+} pm_batch_tuning;
+
+PM_API pm_status pm_batch_create(pm_sim* const* scenes, uint32_t n, pm_batch** out);
+PM_API pm_status pm_batch_destroy(pm_batch* batch);
+/* Advances every scene by nsteps steps. */
+PM_API pm_status pm_batch_step(pm_batch* batch, uint32_t nsteps);
+PM_API pm_status pm_batch_get_tuning(pm_batch* batch, pm_batch_tuning* tuning);
+PM_API pm_status pm_batch_set_tuning(pm_batch* batch, const pm_batch_tuning* tuning);
+/* Coordinate search over the launch shapes: each candidate is timed with CUDA events over
+ * trial_rounds rounds (which advance the scenes like pm_batch_step), the fastest is kept and
+ * returned in best (may be NULL) with its time per round in best_ms (may be NULL). */
+PM_API pm_status pm_batch_autotune(pm_batch* batch, uint32_t trial_rounds, pm_batch_tuning* best, float* best_ms);
+/* The stream the batch issues its work on, for CUDA event timing. */
+PM_API pm_status pm_batch_get_stream(pm_batch* batch, void** stream);
+/* Kernels per round and their names in launch order. */
+PM_API int32_t pm_batch_kernels_per_round(pm_batch* batch);
+PM_API const char* pm_batch_kernel_name(pm_batch* batch, int index);
+/* Runs `rounds` rounds without the graph, timing every kernel with CUDA events; kernel_ms[i]
+ * receives the mean duration of kernel i (n_kernels >= pm_batch_kernels_per_round). */
+PM_API pm_status pm_batch_profile(pm_batch* batch, uint32_t rounds, float* kernel_ms, uint32_t n_kernels);
+
 /* ---- particle-to-grid transfer that allocates nothing --------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc: code running while
  * a CUDA graph is captured, and plug-ins whose host application owns every device allocation.

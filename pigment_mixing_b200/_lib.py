@@ -58,7 +58,24 @@ SIGNATURES = {
     "pm_mlp_loss_grad": [_fp, _fp, _fp, C.c_uint32, _fp, _fp],
     "pm_mlp_infer": [_fp, _fp, C.c_uint32, _fp],
     "pm_p2g_noalloc": [_vp] * 5 + [C.c_uint32, C.c_double, C.c_double, _dp, C.POINTER(C.c_int32)] + [_vp] * 5 + [_up],
+    "pm_batch_create": [C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(C.c_void_p)],
+    "pm_batch_destroy": [_vp],
+    "pm_batch_step": [_vp, C.c_uint32],
+    "pm_batch_get_tuning": [_vp, _vp],
+    "pm_batch_set_tuning": [_vp, _vp],
+    "pm_batch_autotune": [_vp, C.c_uint32, _vp, _fp],
+    "pm_batch_get_stream": [_vp, C.POINTER(C.c_void_p)],
+    "pm_batch_profile": [_vp, C.c_uint32, _fp, C.c_uint32],
 }
+
+
+class BatchTuning(C.Structure):
+    """pm_batch_tuning (include/pigment_mpm.h)."""
+    _fields_ = [(n, C.c_int32) for n in ("flat_threads", "part_ctas_per_sm", "node_ctas_per_sm", "p2g_ctas_per_sm",
+                                         "g2p_ctas_per_sm", "def_ctas_per_sm", "sur_ctas_per_sm", "chunk_rounds")]
+
+    def as_dict(self) -> dict:
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
 
 
 class PMError(RuntimeError):
@@ -85,6 +102,10 @@ def lib() -> C.CDLL:
     L.pm_last_error_message.argtypes = []
     L.pm_kernel_name.restype = C.c_char_p
     L.pm_kernel_name.argtypes = [C.c_void_p, C.c_int]
+    L.pm_batch_kernel_name.restype = C.c_char_p
+    L.pm_batch_kernel_name.argtypes = [C.c_void_p, C.c_int]
+    L.pm_batch_kernels_per_round.restype = C.c_int32
+    L.pm_batch_kernels_per_round.argtypes = [C.c_void_p]
     _lib = L
     return L
 

@@ -376,6 +376,8 @@ pm_status pm_sim::run_steps(uint32_t n, bool use_graph) {
     cur = (cur + (int)done) & 1;
     remaining -= std::min(done, remaining);
     if (done > 0) guard = 0;  // count only regrowths that made no progress
+    if (done == 0 && !h_ctrl->halt)
+      return fail(PM_ERR_STATE, "steps made no progress (the control block holds a batch target)");
     long long want = 0;
     if (h_ctrl->halt) {
       if (++guard > 8) return fail(PM_ERR_CAPACITY, "grid keeps overflowing after regrowth");
@@ -1264,6 +1266,423 @@ pm_status pm_profile_steps(pm_sim* sim, uint32_t nsteps, float* kernel_ms, uint3
   }
   for (auto& e : ev) cudaEventDestroy(e);
   for (int i = 0; i < K; ++i) kernel_ms[i] = done_steps ? (float)(acc[i] / done_steps) : 0.f;
+  return st;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// batched scenes
+// ------------------------------------------------------------------------------------------
+struct pm_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<pm_sim*> sims;
+  std::vector<SceneDev> h_sd;
+  SceneDev* d_sd = nullptr;
+  std::vector<int> h_off;
+  int* d_off = nullptr;
+  std::vector<uint32_t> par_base, target, auto_frame;
+  BatchLaunch L;
+  pm_batch_tuning tune{};
+  int occ_p2g = 1, occ_g2p = 1, occ_def = 1;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_dirty = true;
+
+  ~pm_batch() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (d_sd) cudaFree(d_sd);
+    if (d_off) cudaFree(d_off);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  int ns() const { return (int)sims.size(); }
+  pm_status upload_tables();
+  pm_status capture();
+  pm_status begin(uint32_t nsteps);
+  pm_status poll(bool& all_done, bool& progress, bool allow_regrow);
+  pm_status finish();
+  pm_status run_rounds(uint32_t n);
+};
+
+namespace {
+// Splits `total` CTAs over the scenes in proportion to w (at least one each); returns offsets.
+void proportional(const std::vector<double>& w, int total, std::vector<int>& off) {
+  const int n = (int)w.size();
+  double sum = 0.0;
+  for (double x : w) sum += x;
+  off.assign(n + 1, 0);
+  for (int s = 0; s < n; ++s) {
+    const int c = std::max(1, (int)std::lround(sum > 0.0 ? total * w[s] / sum : (double)total / n));
+    off[s + 1] = off[s] + c;
+  }
+}
+}  // namespace
+
+// Rebuilds the scene table (constants and buffers of both parities) and the CTA partitions,
+// uploads them, and marks the graph for recapture when a launch size changed.
+pm_status pm_batch::upload_tables() {
+  const int n = ns();
+  const int sms = num_sms() > 0 ? num_sms() : 148;
+  h_sd.assign(n, SceneDev{});
+  std::vector<double> wp(n), wn(n);
+  std::vector<int> scan(n + 1, 0);
+  bool sur = false;
+  for (int s = 0; s < n; ++s) {
+    pm_sim* m = sims[s];
+    m->fill_params();
+    h_sd[s].P = m->P;
+    h_sd[s].B[0] = m->bufs(0);
+    h_sd[s].B[1] = m->bufs(1);
+    h_sd[s].par_base = par_base[s];
+    wp[s] = (double)std::max<uint32_t>(m->np, 1);
+    wn[s] = (double)std::max(m->P.node_cap, 1);
+    scan[s + 1] = scan[s] + scan_blocks_for(m->P.node_cap);
+    sur = sur || m->P.return_map == 1;
+  }
+  std::vector<int> unit(n + 1), part, node, p2g, g2p, def, surv;
+  for (int s = 0; s <= n; ++s) unit[s] = s;
+  proportional(wp, sms * tune.part_ctas_per_sm, part);
+  proportional(wn, sms * tune.node_ctas_per_sm, node);
+  proportional(wp, sms * tune.p2g_ctas_per_sm, p2g);
+  proportional(wp, sms * tune.g2p_ctas_per_sm, g2p);
+  proportional(wp, sms * tune.def_ctas_per_sm, def);
+  proportional(wp, sms * tune.sur_ctas_per_sm, surv);
+  const std::vector<int>* tabs[] = {&unit, &part, &node, &scan, &p2g, &g2p, &def, &surv};
+  h_off.clear();
+  for (auto* t : tabs) h_off.insert(h_off.end(), t->begin(), t->end());
+  if (!d_sd) CK(cudaMalloc(&d_sd, sizeof(SceneDev) * (size_t)n));
+  if (!d_off) CK(cudaMalloc(&d_off, sizeof(int) * 8 * (size_t)(n + 1)));
+  CK(cudaMemcpyAsync(d_sd, h_sd.data(), sizeof(SceneDev) * (size_t)n, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_off, h_off.data(), sizeof(int) * h_off.size(), cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  BatchLaunch nl;
+  nl.sd = d_sd;
+  nl.ns = n;
+  const int* o = d_off;
+  nl.off_unit = o; o += n + 1;
+  nl.off_part = o; o += n + 1;
+  nl.off_node = o; o += n + 1;
+  nl.off_scan = o; o += n + 1;
+  nl.off_p2g = o; o += n + 1;
+  nl.off_g2p = o; o += n + 1;
+  nl.off_def = o; o += n + 1;
+  nl.off_sur = o;
+  nl.n_part = part[n]; nl.n_node = node[n]; nl.n_scan = scan[n]; nl.n_p2g = p2g[n];
+  nl.n_g2p = g2p[n]; nl.n_def = def[n]; nl.n_sur = surv[n];
+  nl.flat_threads = tune.flat_threads;
+  nl.surrogate = sur;
+  if (std::memcmp(&nl, &L, sizeof(BatchLaunch)) != 0) graph_dirty = true;
+  L = nl;
+  return PM_OK;
+}
+
+pm_status pm_batch::capture() {
+  if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  launch_step_batched(L, stream, nullptr);
+  cudaError_t e = cudaStreamEndCapture(stream, &g);
+  if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(e));
+  graph_dirty = false;
+  return PM_OK;
+}
+
+// Sets every scene's target to its current step + nsteps and records its buffer parity.
+pm_status pm_batch::begin(uint32_t nsteps) {
+  CK(cudaSetDevice(device));
+  const int n = ns();
+  par_base.assign(n, 0);
+  target.assign(n, 0);
+  auto_frame.assign(n, 0);
+  for (int s = 0; s < n; ++s) {
+    pm_sim* m = sims[s];
+    if (!m->prepared) return fail(PM_ERR_STATE, "every scene of a batch must be prepared");
+    CK(cudaStreamSynchronize(m->stream));
+    pm_status st = m->sync_ctrl();
+    if (st != PM_OK) return st;
+    if (m->h_ctrl->halt) return fail(PM_ERR_STATE, "a scene is halted; step it once on its own first");
+    par_base[s] = (uint32_t)(m->cur - (int)(m->h_ctrl->step & 1u)) & 1u;
+    target[s] = m->h_ctrl->step + nsteps;
+    m->h_ctrl->target_step = target[s];
+    // a batch step is an advance(): frame bookkeeping after every step (as pm_advance does)
+    auto_frame[s] = m->h_ctrl->auto_frame;
+    m->h_ctrl->auto_frame = 1;
+    st = m->push_ctrl();
+    if (st != PM_OK) return st;
+  }
+  return upload_tables();
+}
+
+// Reads every control block; regrows halted scenes (when allowed).  all_done: every scene at
+// its target; progress: some scene advanced since the previous poll.
+pm_status pm_batch::poll(bool& all_done, bool& progress, bool allow_regrow) {
+  const int n = ns();
+  for (int s = 0; s < n; ++s)
+    CK(cudaMemcpyAsync(sims[s]->h_ctrl, sims[s]->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  all_done = true;
+  progress = false;
+  bool regrown = false;
+  for (int s = 0; s < n; ++s) {
+    pm_sim* m = sims[s];
+    if (m->h_ctrl->step != m->host_step) progress = true;
+    m->host_step = m->h_ctrl->step;
+    if (m->h_ctrl->step < target[s]) all_done = false;
+    if (m->h_ctrl->halt) {
+      if (!allow_regrow) return fail(PM_ERR_CAPACITY, "grid capacity reached while profiling a batch");
+      const long long want = (long long)m->h_ctrl->need_bricks * 2 + 64;
+      if (want * kBrickNodes > 0x7ffffff0LL) return fail(PM_ERR_CAPACITY, "grid would exceed 2^31 nodes");
+      pm_status st = m->alloc_grid((int)want);
+      if (st != PM_OK) return st;
+      ++m->regrowths;
+      m->h_ctrl->halt = 0;
+      m->h_ctrl->error_flags &= ~(uint32_t)E_CAPACITY;
+      st = m->push_ctrl();
+      if (st != PM_OK) return st;
+      regrown = true;
+    } else if (!all_done && m->h_ctrl->step < target[s] && m->h_ctrl->n_bricks > 0.8 * m->brick_cap) {
+      pm_status st = m->alloc_grid(m->h_ctrl->n_bricks * 2 + 64);
+      if (st != PM_OK) return st;
+      ++m->regrowths;
+      regrown = true;
+    }
+  }
+  if (regrown) return upload_tables();
+  return PM_OK;
+}
+
+// Leaves every scene ready for per-scene calls: host step and parity mirrored, target cleared.
+pm_status pm_batch::finish() {
+  for (int s = 0; s < ns(); ++s) {
+    pm_sim* m = sims[s];
+    pm_status st = m->sync_ctrl();
+    if (st != PM_OK) return st;
+    m->host_step = m->h_ctrl->step;
+    m->cur = (int)((m->h_ctrl->step + par_base[s]) & 1u);
+    m->h_ctrl->target_step = 0;
+    m->h_ctrl->idle = 0;
+    m->h_ctrl->auto_frame = auto_frame[s];
+    st = m->push_ctrl();
+    if (st != PM_OK) return st;
+  }
+  return PM_OK;
+}
+
+// Replays the one-round graph until every scene has reached its target (at most `n` rounds per
+// scene plus the rounds a regrown scene sat out).
+pm_status pm_batch::run_rounds(uint32_t n) {
+  uint32_t remaining = n;
+  int stalls = 0;
+  uint64_t launched = 0;
+  const uint64_t limit = 4ull * n + 4096;  // regrowth re-runs are rare; anything beyond is a fault
+  while (true) {
+    if (launched > limit) return fail(PM_ERR_STATE, "batch rounds exceed the expected count");
+    if (graph_dirty) { pm_status st = capture(); if (st != PM_OK) return st; }
+    const uint32_t r = std::max<uint32_t>(1, std::min<uint32_t>(remaining, (uint32_t)std::max(1, tune.chunk_rounds)));
+    for (uint32_t k = 0; k < r; ++k) CK(cudaGraphLaunch(gexec, stream));
+    CK(cudaGetLastError());
+    launched += r;
+    remaining = remaining > r ? remaining - r : 0;
+    bool done = false, progress = false;
+    pm_status st = poll(done, progress, true);
+    if (st != PM_OK) return st;
+    if (done) return PM_OK;
+    stalls = progress ? 0 : stalls + 1;
+    if (stalls > 8) return fail(PM_ERR_CAPACITY, "batch makes no progress after regrowth");
+    if (remaining == 0) {  // scenes that sat rounds out still owe steps
+      uint32_t owe = 0;
+      for (int s = 0; s < ns(); ++s)
+        owe = std::max(owe, target[s] > sims[s]->h_ctrl->step ? target[s] - sims[s]->h_ctrl->step : 0u);
+      remaining = owe;
+    }
+  }
+}
+
+extern "C" {
+
+pm_status pm_batch_create(pm_sim* const* scenes, uint32_t n, pm_batch** out) {
+  if (!scenes || !out || n == 0) return fail(PM_ERR_INVALID, "need at least one scene and an out pointer");
+  *out = nullptr;
+  const int dev = scenes[0] ? scenes[0]->device : 0;
+  for (uint32_t s = 0; s < n; ++s) {
+    if (!scenes[s]) return fail(PM_ERR_INVALID, "NULL scene");
+    if (scenes[s]->device != dev) return fail(PM_ERR_INVALID, "all scenes of a batch must be on one device");
+    if (!scenes[s]->prepared) return fail(PM_ERR_STATE, "every scene of a batch must be prepared");
+    for (uint32_t t = 0; t < s; ++t)
+      if (scenes[t] == scenes[s]) return fail(PM_ERR_INVALID, "a scene appears twice in the batch");
+  }
+  CK(cudaSetDevice(dev));
+  pm_batch* b = new pm_batch();
+  b->device = dev;
+  b->sims.assign(scenes, scenes + n);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete b;
+    return fail(PM_ERR_CUDA, "stream");
+  }
+  batched_occupancy(b->occ_p2g, b->occ_g2p, b->occ_def);
+  b->tune.flat_threads = 256;
+  b->tune.part_ctas_per_sm = 8;
+  b->tune.node_ctas_per_sm = 8;
+  b->tune.p2g_ctas_per_sm = b->occ_p2g;
+  b->tune.g2p_ctas_per_sm = b->occ_g2p;
+  b->tune.def_ctas_per_sm = b->occ_def;
+  b->tune.sur_ctas_per_sm = 8;
+  b->tune.chunk_rounds = 64;
+  *out = b;
+  return PM_OK;
+}
+
+pm_status pm_batch_destroy(pm_batch* b) {
+  if (!b) return PM_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  delete b;
+  return PM_OK;
+}
+
+pm_status pm_batch_step(pm_batch* b, uint32_t nsteps) {
+  if (!b) return fail(PM_ERR_INVALID, "NULL batch");
+  if (nsteps == 0) return PM_OK;
+  pm_status st = b->begin(nsteps);
+  if (st != PM_OK) return st;
+  st = b->run_rounds(nsteps);
+  pm_status st2 = b->finish();
+  return st != PM_OK ? st : st2;
+}
+
+pm_status pm_batch_get_tuning(pm_batch* b, pm_batch_tuning* t) {
+  if (!b || !t) return fail(PM_ERR_INVALID, "NULL argument");
+  *t = b->tune;
+  return PM_OK;
+}
+
+pm_status pm_batch_set_tuning(pm_batch* b, const pm_batch_tuning* t) {
+  if (!b || !t) return fail(PM_ERR_INVALID, "NULL argument");
+  if (t->flat_threads != 128 && t->flat_threads != 256 && t->flat_threads != 512)
+    return fail(PM_ERR_INVALID, "flat_threads must be 128, 256 or 512");
+  const int32_t v[] = {t->part_ctas_per_sm, t->node_ctas_per_sm, t->p2g_ctas_per_sm, t->g2p_ctas_per_sm,
+                       t->def_ctas_per_sm, t->sur_ctas_per_sm};
+  for (int32_t x : v)
+    if (x < 1 || x > 64) return fail(PM_ERR_INVALID, "CTAs per SM must be in [1, 64]");
+  if (t->chunk_rounds < 1 || t->chunk_rounds > 4096) return fail(PM_ERR_INVALID, "chunk_rounds must be in [1, 4096]");
+  b->tune = *t;
+  b->graph_dirty = true;
+  return PM_OK;
+}
+
+pm_status pm_batch_get_stream(pm_batch* b, void** stream) {
+  if (!b || !stream) return fail(PM_ERR_INVALID, "NULL argument");
+  *stream = (void*)b->stream;
+  return PM_OK;
+}
+
+int32_t pm_batch_kernels_per_round(pm_batch* b) {
+  if (!b) return 0;
+  bool sur = false;
+  for (pm_sim* m : b->sims) sur = sur || (m->return_map == PM_RETURN_MAP_SURROGATE && m->has_mlp && m->d_q);
+  return batched_kernels_per_step(sur);
+}
+
+const char* pm_batch_kernel_name(pm_batch* b, int index) {
+  if (!b) return "";
+  bool sur = false;
+  for (pm_sim* m : b->sims) sur = sur || (m->return_map == PM_RETURN_MAP_SURROGATE && m->has_mlp && m->d_q);
+  return batched_kernel_name(index, sur);
+}
+
+pm_status pm_batch_profile(pm_batch* b, uint32_t rounds, float* kernel_ms, uint32_t n_kernels) {
+  if (!b || !kernel_ms) return fail(PM_ERR_INVALID, "NULL argument");
+  if (rounds == 0) return PM_OK;
+  pm_status st = b->begin(rounds);
+  if (st != PM_OK) return st;
+  const int K = batched_kernels_per_step(b->L.surrogate);
+  if ((int)n_kernels < K) { b->finish(); return fail(PM_ERR_INVALID, "kernel_ms needs kernels_per_round entries"); }
+  std::vector<cudaEvent_t> ev(K + 1);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  std::vector<double> acc(K, 0.0);
+  for (uint32_t r = 0; r < rounds && st == PM_OK; ++r) {
+    launch_step_batched(b->L, b->stream, ev.data());
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) { st = fail(PM_ERR_CUDA, "profiled round failed"); break; }
+    for (int i = 0; i < K; ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+      acc[i] += ms;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int i = 0; i < K; ++i) kernel_ms[i] = (float)(acc[i] / rounds);
+  if (st == PM_OK) {  // scenes that halted while profiled are regrown and brought to the target
+    bool done = false, progress = false;
+    st = b->poll(done, progress, true);
+    if (st == PM_OK && !done) st = b->run_rounds(0);
+  }
+  pm_status st2 = b->finish();
+  return st != PM_OK ? st : st2;
+}
+
+pm_status pm_batch_autotune(pm_batch* b, uint32_t trial_rounds, pm_batch_tuning* best, float* best_ms) {
+  if (!b) return fail(PM_ERR_INVALID, "NULL batch");
+  if (trial_rounds == 0) trial_rounds = 4;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto trial = [&](const pm_batch_tuning& t, float& ms) -> pm_status {
+    b->tune = t;
+    b->graph_dirty = true;
+    pm_status st = b->begin(trial_rounds + 1);
+    if (st != PM_OK) return st;
+    if ((st = b->capture()) != PM_OK) return st;
+    CK(cudaGraphLaunch(b->gexec, b->stream));  // warm-up round
+    CK(cudaEventRecord(e0, b->stream));
+    for (uint32_t r = 0; r < trial_rounds; ++r) CK(cudaGraphLaunch(b->gexec, b->stream));
+    CK(cudaEventRecord(e1, b->stream));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    ms /= (float)trial_rounds;
+    bool done = false, progress = false;
+    st = b->poll(done, progress, true);
+    if (st == PM_OK && !done) st = b->run_rounds(0);
+    pm_status st2 = b->finish();
+    return st != PM_OK ? st : st2;
+  };
+  pm_batch_tuning cur = b->tune;
+  float cur_ms = 0.f;
+  pm_status st = trial(cur, cur_ms);
+  // coordinate search: one launch-shape parameter at a time, two passes
+  static int32_t pm_batch_tuning::*const kField[7] = {
+      &pm_batch_tuning::flat_threads,    &pm_batch_tuning::part_ctas_per_sm, &pm_batch_tuning::node_ctas_per_sm,
+      &pm_batch_tuning::p2g_ctas_per_sm, &pm_batch_tuning::g2p_ctas_per_sm, &pm_batch_tuning::def_ctas_per_sm,
+      &pm_batch_tuning::sur_ctas_per_sm};
+  for (int pass = 0; pass < 2 && st == PM_OK; ++pass) {
+    for (int field = 0; field < 7 && st == PM_OK; ++field) {
+      std::vector<int32_t> cand;
+      switch (field) {
+        case 0: cand = {128, 256, 512}; break;
+        case 3: cand = {b->occ_p2g, 2 * b->occ_p2g}; break;
+        case 4: cand = {b->occ_g2p, 2 * b->occ_g2p}; break;
+        case 5: cand = {b->occ_def, 2 * b->occ_def}; break;
+        default: cand = {4, 8, 16}; break;
+      }
+      if (field == 6 && !b->L.surrogate) continue;
+      for (int32_t v : cand) {
+        if (v == cur.*kField[field] || st != PM_OK) continue;
+        pm_batch_tuning tt = cur;
+        tt.*kField[field] = v;
+        float ms = 0.f;
+        st = trial(tt, ms);
+        if (st == PM_OK && ms < cur_ms) { cur = tt; cur_ms = ms; }
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->tune = cur;
+  b->graph_dirty = true;
+  if (best) *best = cur;
+  if (best_ms) *best_ms = cur_ms;
   return st;
 }
 

@@ -166,6 +166,8 @@ struct Ctrl {
   uint32_t newton_solves;  // particles that needed the Perzyna consistency solve this step
   uint32_t sur_accept;     // surrogate estimates that passed the consistency check
   uint32_t slog_n;         // samples written to the log (cumulative)
+  uint32_t target_step;    // batches: the scene idles once step reaches this (0 = no target)
+  uint32_t idle;           // set by the prologue: this round is skipped for the scene
   uint32_t pad0;
   // objects
   int n_plates, n_objects, knife;  // knife: index into objects or -1
@@ -196,6 +198,34 @@ struct Bufs {
   float* qx;              // q_cap x 10 surrogate inputs
   float* qy;              // q_cap x 6 surrogate outputs
 };
+
+// One scene of a batch as the batched kernels see it: its constants and both buffer parities.
+// The parity of a step is (ctrl->step + par_base) & 1, so scenes that idle or halt for a round
+// keep their own parity.
+struct SceneDev {
+  Params P;
+  Bufs B[2];
+  uint32_t par_base;
+  uint32_t pad[3];
+};
+
+__device__ __forceinline__ int scene_parity(const SceneDev& d) {
+  return (int)((d.B[0].ctrl->step + d.par_base) & 1u);
+}
+
+// Static partition of a batched launch: scene s owns CTAs [off[s], off[s+1]).  Returns the
+// scene of this CTA and the CTA's index and count within the scene.
+__device__ __forceinline__ void batch_slot(const int* __restrict__ off, int ns, int& s, int& blk, int& nblk) {
+  const int b = (int)blockIdx.x;
+  int lo = 0, hi = ns;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= b) lo = mid; else hi = mid;
+  }
+  s = lo;
+  blk = b - off[lo];
+  nblk = off[lo + 1] - off[lo];
+}
 
 // Order-preserving float <-> int key (min/max of floats through integer atomics).
 __host__ __device__ inline int fkey(float f) {

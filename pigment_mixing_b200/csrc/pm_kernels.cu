@@ -110,10 +110,13 @@ __device__ void grid_box_from_aabb(const Params& P, Ctrl* c) {
   c->n_nodes = (int)nbricks * kBrickNodes;
 }
 
-__global__ void k_prologue(Params P, Bufs B) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void d_prologue(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
+  if (threadIdx.x != 0 || blk_ != 0) return;
   Ctrl* c = B.ctrl;
   if (c->halt) return;
+  // a scene of a batch that has reached its target step sits this round out
+  c->idle = (c->target_step != 0u && c->step >= c->target_step) ? 1u : 0u;
+  if (c->idle) return;
   // updateDt (update_dt.cpp:5-41)
   float m2f = __uint_as_float(c->max_v2);
   double ms = sqrt((double)m2f);
@@ -157,6 +160,14 @@ __global__ void k_prologue(Params P, Bufs B) {
   c->newton_solves = 0;
   c->sur_accept = 0;
 }
+__global__ void k_prologue(Params P, Bufs B) { d_prologue(P, B, blockIdx.x, gridDim.x); }
+__global__ void kb_prologue(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_prologue(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
+
 
 // quaternion helpers (w, x, y, z)
 __device__ void q_to_rot(const double q[4], double R[9]) {
@@ -259,10 +270,10 @@ __device__ void move_knife(const Params& P, ObjDev& o, double dt) {
   }
 }
 
-__global__ void k_epilogue(Params P, Bufs B) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void d_epilogue(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
+  if (threadIdx.x != 0 || blk_ != 0) return;
   Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   double dt = c->dt;
   // moveObjects (simulation.cpp:284-291): plates, then the spatula
   for (int i = 0; i < c->n_plates; ++i) {  // object_plate.hpp:136-162
@@ -280,6 +291,14 @@ __global__ void k_epilogue(Params P, Bufs B) {
     if (P.frame_dt * (double)(c->frame + 1) - c->time < P.min_dt * 1.1) { c->frame += 1; c->frames_done += 1; }
   }
 }
+__global__ void k_epilogue(Params P, Bufs B) { d_epilogue(P, B, blockIdx.x, gridDim.x); }
+__global__ void kb_epilogue(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_epilogue(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
+
 
 // ------------------------------------------------------------------------------------------
 // counting sort by cell
@@ -294,26 +313,34 @@ __device__ __forceinline__ void brick_coords(int b, const Ctrl* c, int& bx, int&
 
 // Zeroes the per-node counters of the counting sort (the grid records are cleared per brick by
 // k_clear_bricks once the occupied bricks are known).
-__global__ void k_clear(Params P, Bufs B) {
+__device__ __forceinline__ void d_clear(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   const int nn = c->n_nodes;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn + 2; i += stride) B.cell[i] = 0u;
+  const int stride = nblk_ * blockDim.x;
+  for (int i = blk_ * blockDim.x + threadIdx.x; i < nn + 2; i += stride) B.cell[i] = 0u;
 }
+__global__ void k_clear(Params P, Bufs B) { d_clear(P, B, blockIdx.x, gridDim.x); }
+__global__ void kb_clear(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_clear(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
+
 
 // After the scan: a brick is touched this step when one of the bricks b - d, d in {0,1}^3, holds
 // particles (a particle's 3x3x3 stencil spans its own brick and the next one on each axis).
 // One warp per brick: lanes 0..7 test the eight source bricks, then the warp zeroes the brick's
 // 64 accumulated records and MUSL records and stores the flag that k_grid_update reads.  Only
 // touched bricks are ever read by the transfers, so untouched ones are left as they are.
-__global__ void k_clear_bricks(Params P, Bufs B) {
+__device__ __forceinline__ void d_clear_bricks(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   const int nbr = c->n_bricks, lane = threadIdx.x & 31;
-  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int warps = nblk_ * (blockDim.x >> 5);
   const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); b < nbr; b += warps) {
+  for (int b = blk_ * (blockDim.x >> 5) + (threadIdx.x >> 5); b < nbr; b += warps) {
     bool occ = false;
     if (lane < 8) {
       int bx, by, bz;
@@ -337,6 +364,14 @@ __global__ void k_clear_bricks(Params P, Bufs B) {
     }
   }
 }
+__global__ void k_clear_bricks(Params P, Bufs B) { d_clear_bricks(P, B, blockIdx.x, gridDim.x); }
+__global__ void kb_clear_bricks(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_clear_bricks(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
+
 
 __device__ __forceinline__ uint32_t brick_key(const int c[3], const Ctrl* ctrl) {
   int bx = c[0] >> 2, by = c[1] >> 2, bz = c[2] >> 2;
@@ -344,14 +379,14 @@ __device__ __forceinline__ uint32_t brick_key(const int c[3], const Ctrl* ctrl) 
   return (uint32_t)(((bx * ctrl->nb[1] + by) * ctrl->nb[2] + bz) * kBrickNodes + lx * 16 + ly * 4 + lz);
 }
 
-__global__ void k_count(Params P, Bufs B) {
+__device__ __forceinline__ void d_count(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   const int np = P.np, S = P.np_stride;
   const uint32_t inactive_key = (uint32_t)c->n_nodes;
-  const int stride = gridDim.x * blockDim.x;
+  const int stride = nblk_ * blockDim.x;
   bool range_err = false;
-  for (int base = blockIdx.x * blockDim.x; base < np; base += stride) {
+  for (int base = blk_ * blockDim.x; base < np; base += stride) {
     int p = base + threadIdx.x;
     bool valid = p < np;
     uint32_t key = 0xffffffffu;
@@ -384,6 +419,14 @@ __global__ void k_count(Params P, Bufs B) {
   }
   if (range_err) atomicOr(&B.ctrl->error_flags, (uint32_t)E_INDEX_RANGE);
 }
+__global__ void k_count(Params P, Bufs B) { d_count(P, B, blockIdx.x, gridDim.x); }
+__global__ void kb_count(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_count(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
+
 
 // Exclusive scan of cell[0 .. n_nodes+1) in 4096-entry blocks.
 constexpr int kScanThreads = 1024;
@@ -413,11 +456,11 @@ __device__ __forceinline__ uint32_t block_incl_scan(uint32_t v, uint32_t* warp_s
   return v;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_local(Params P, Bufs B) {
+__device__ __forceinline__ void d_scan_local(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   const int n = c->n_nodes + 1;
-  const int b0 = blockIdx.x * kScanBlock;
+  const int b0 = blk_ * kScanBlock;
   if (b0 >= n) return;
   __shared__ uint32_t ws[32];
   uint32_t v[kScanPer];
@@ -432,12 +475,20 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_local(Params P, Bufs B) {
     if (i0 + k < n) B.cell[i0 + k] = run;
     run += v[k];
   }
-  if (threadIdx.x == kScanThreads - 1) B.scan_part[blockIdx.x] = incl;
+  if (threadIdx.x == kScanThreads - 1) B.scan_part[blk_] = incl;
+}
+__global__ void __launch_bounds__(kScanThreads) k_scan_local(Params P, Bufs B) { d_scan_local(P, B, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kScanThreads) kb_scan_local(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_scan_local(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_top(Params P, Bufs B) {
+
+__device__ __forceinline__ void d_scan_top(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   const int n = c->n_nodes + 1;
   const int nblk = (n + kScanBlock - 1) / kScanBlock;
   __shared__ uint32_t ws[32];
@@ -456,24 +507,48 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_top(Params P, Bufs B) {
   }
   if (threadIdx.x == 0) B.cell[n] = carry_s;  // total = np
 }
+__global__ void __launch_bounds__(kScanThreads) k_scan_top(Params P, Bufs B) { d_scan_top(P, B, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kScanThreads) kb_scan_top(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_scan_top(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_add(Params P, Bufs B) {
+
+__device__ __forceinline__ void d_scan_add(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   const int n = c->n_nodes + 1;
-  const int b0 = blockIdx.x * kScanBlock;
-  if (b0 >= n || blockIdx.x == 0) return;
-  const uint32_t off = B.scan_part[blockIdx.x];
+  const int b0 = blk_ * kScanBlock;
+  if (b0 >= n || blk_ == 0) return;
+  const uint32_t off = B.scan_part[blk_];
   for (int i = b0 + threadIdx.x; i < min(b0 + kScanBlock, n); i += kScanThreads) B.cell[i] += off;
 }
+__global__ void __launch_bounds__(kScanThreads) k_scan_add(Params P, Bufs B) { d_scan_add(P, B, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kScanThreads) kb_scan_add(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_scan_add(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
 
-__global__ void k_scatter(Params P, Bufs B) {
+
+__device__ __forceinline__ void d_scatter(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
-  const int stride = gridDim.x * blockDim.x;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.np; p += stride)
+  if (c->halt || c->idle) return;
+  const int stride = nblk_ * blockDim.x;
+  for (int p = blk_ * blockDim.x + threadIdx.x; p < P.np; p += stride)
     B.sorted[B.cell[B.key[p]] + B.rank[p]] = (uint32_t)p;
 }
+__global__ void k_scatter(Params P, Bufs B) { d_scatter(P, B, blockIdx.x, gridDim.x); }
+__global__ void kb_scatter(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_scatter(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
+
 
 // ------------------------------------------------------------------------------------------
 // P2G: warp per cell, lane per stencil node, shared 6x6x6 tile per brick
@@ -521,9 +596,9 @@ __device__ __forceinline__ int local_cell(const AxisW aw[3], const Ctrl* c, int 
 // walks the runs of equal cells in its 32 particles (found with a ballot) and, for each run,
 // lane l < 27 accumulates the run's particles into stencil node l in registers and adds the
 // sums once to the brick's shared 6x6x6 tile.  Block barriers only around the tile.
-__global__ void __launch_bounds__(kThreads) k_p2g(Params P, Bufs B) {
+__device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* tile = reinterpret_cast<float*>(smem_raw);                       // [kP2GCh][216]
   StageP2G* stw = reinterpret_cast<StageP2G*>(tile + kP2GCh * kTileNodes);  // [kWarps][32]
@@ -535,7 +610,7 @@ __global__ void __launch_bounds__(kThreads) k_p2g(Params P, Bufs B) {
   const float D = P.apicD, dx = P.dx;
   const bool apic = P.flip_ratio < 0.f;
   const int nbr = c->n_bricks;
-  for (int b = blockIdx.x; b < nbr; b += gridDim.x) {
+  for (int b = blk_; b < nbr; b += nblk_) {
     const uint32_t ps = B.cell[(size_t)b * kBrickNodes], pe = B.cell[(size_t)(b + 1) * kBrickNodes];
     if (ps == pe) continue;
     int bx, by, bz;
@@ -643,6 +718,14 @@ __global__ void __launch_bounds__(kThreads) k_p2g(Params P, Bufs B) {
     __syncthreads();
   }
 }
+__global__ void __launch_bounds__(kThreads) k_p2g(Params P, Bufs B) { d_p2g(P, B, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kThreads) kb_p2g(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_p2g(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
+
 
 // ------------------------------------------------------------------------------------------
 // grid update with collisions
@@ -825,16 +908,16 @@ __device__ void boundary_collision(const Ctrl* c, float dtf, float dx, float Xi_
   }
 }
 
-__global__ void k_grid_update(Params P, Bufs B) {
+__device__ __forceinline__ void d_grid_update(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   const int nn = c->n_nodes;
   const float dtf = (float)c->dt;
   const float dtv = dtf * P.particle_volume;
   const float dtg[3] = {dtf * P.gravity[0], dtf * P.gravity[1], dtf * P.gravity[2]};
-  const int stride = gridDim.x * blockDim.x;
+  const int stride = nblk_ * blockDim.x;
   uint32_t err = 0;
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += stride) {
+  for (int n = blk_ * blockDim.x + threadIdx.x; n < nn; n += stride) {
     if (!B.btouch[n >> 6]) continue;  // no particle stencil reaches this brick: record is stale
     float4* rec = B.grid + (size_t)n * 4;
     float4 r0 = rec[0];
@@ -870,6 +953,14 @@ __global__ void k_grid_update(Params P, Bufs B) {
   }
   if (err) atomicOr(&B.ctrl->error_flags, err);
 }
+__global__ void k_grid_update(Params P, Bufs B) { d_grid_update(P, B, blockIdx.x, gridDim.x); }
+__global__ void kb_grid_update(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_grid_update(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
+
 
 // ------------------------------------------------------------------------------------------
 // G2P + mixing + MUSL (velocity update and re-scatter)
@@ -898,9 +989,9 @@ __device__ __forceinline__ float smooth_step(float e0, float e1, float x) {  // 
 // gathers G2P for particle i, writes its new state in sorted order and stages its MUSL data; the
 // warp then scatters the staged particles run by run of equal cells, lane l < 27 owning stencil
 // node l, into the brick's shared MUSL tile, flushed once per brick.
-__global__ void __launch_bounds__(kThreads, 5) k_g2p_musl(Params P, Bufs B) {
+__device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* tile = reinterpret_cast<float4*>(smem_raw);              // [216][4]
   float* mtile = reinterpret_cast<float*>(tile + 4 * kTileNodes);  // [4][216]
@@ -926,7 +1017,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_g2p_musl(Params P, Bufs B) {
   }
   const float dyn = P.D_max * time_factor;
   const int nbr = c->n_bricks;
-  for (int b = blockIdx.x; b < nbr; b += gridDim.x) {
+  for (int b = blk_; b < nbr; b += nblk_) {
     const uint32_t ps = B.cell[(size_t)b * kBrickNodes], pe = B.cell[(size_t)(b + 1) * kBrickNodes];
     if (ps == pe) continue;
     int bx, by, bz;
@@ -1094,6 +1185,14 @@ __global__ void __launch_bounds__(kThreads, 5) k_g2p_musl(Params P, Bufs B) {
     __syncthreads();
   }
 }
+__global__ void __launch_bounds__(kThreads, 5) k_g2p_musl(Params P, Bufs B) { d_g2p_musl(P, B, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kThreads, 5) kb_g2p_musl(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_g2p_musl(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
+
 
 // ------------------------------------------------------------------------------------------
 // FP64 3x3 SVD (one-sided Jacobi, Hestenes) -- sigma >= 0, U, V orthogonal
@@ -1450,9 +1549,9 @@ __device__ __forceinline__ void finish_F_tau(const Params& P, const double* U, c
   tau[3] = (float)T(0, 1); tau[4] = (float)T(0, 2); tau[5] = (float)T(1, 2);
 }
 
-__global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) {
+__device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   const int S = P.np_stride, np = P.np;
   const double dt = c->dt;
   const float dtf = (float)dt;
@@ -1460,9 +1559,9 @@ __global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) {
   uint32_t err = 0, plastic = 0, nact = 0, niters = 0, nsolves = 0;
   float maxv2 = 0.f;
   int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
-  const int stride = gridDim.x * blockDim.x;
+  const int stride = nblk_ * blockDim.x;
   const float fr = P.flip_ratio;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
+  for (int i = blk_ * blockDim.x + threadIdx.x; i < np; i += stride) {
     const uint32_t o = B.sorted[i];
     const uint32_t meta = B.meta_in[o];
     float* po = B.pout;
@@ -1638,6 +1737,14 @@ __global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) {
     if (red_u[0][3]) atomicOr(&cw->error_flags, red_u[0][3]);
   }
 }
+__global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) { d_defgrad(P, B, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kThreads, 5) kb_defgrad(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_defgrad(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
+
 
 // Surrogate pass: each queued particle turns the network's plastic strain into an estimate of
 // the consistency parameter along its flow direction and checks it against the Perzyna
@@ -1645,14 +1752,14 @@ __global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) {
 // drop to the plain Newton solve -- continued from the estimate, or restarted from the
 // reference's initial guess when sur_fallback_plain is set.  The final F, stress, eps_pl_dev and
 // delta_gamma are written as the plain path writes them.
-__global__ void __launch_bounds__(128) k_sur_finish(Params P, Bufs B) {
+__device__ __forceinline__ void d_sur_finish(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
-  if (c->halt) return;
+  if (c->halt || c->idle) return;
   const uint32_t n = min(c->q_n, P.q_cap);
   const double dt = c->dt;
   const int S = P.np_stride;
   uint32_t err = 0, iters = 0, accepted = 0;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+  for (uint32_t k = blk_ * blockDim.x + threadIdx.x; k < n; k += nblk_ * blockDim.x) {
     const SurQ& r = B.q[k];
     const float* y = B.qy + (size_t)k * 6;
     double pd = 0.0, pr = 0.0;
@@ -1691,6 +1798,14 @@ __global__ void __launch_bounds__(128) k_sur_finish(Params P, Bufs B) {
     if (er) atomicOr(&B.ctrl->error_flags, er);
   }
 }
+__global__ void __launch_bounds__(128) k_sur_finish(Params P, Bufs B) { d_sur_finish(P, B, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(128) kb_sur_finish(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d_ = sd[s_];
+  d_sur_finish(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+}
+
 
 // Reductions over the current particle state (prepare time): max |v|^2, AABB, active count.
 __global__ void __launch_bounds__(kThreads) k_reduce_state(Params P, const float* pcur, const uint32_t* meta, Ctrl* cw) {
@@ -1796,6 +1911,10 @@ cudaError_t launch_init(int device) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_p2g, k_p2g, kThreads, p2g_smem_bytes());
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_g2p, k_g2p_musl, kThreads, g2p_smem_bytes());
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_def, k_defgrad, kThreads, 0);
+  e = cudaFuncSetAttribute(kb_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem_bytes());
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(kb_g2p_musl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes());
+  if (e != cudaSuccess) return e;
   e = mlp_init();
   if (e != cudaSuccess) return e;
   if (g_occ_p2g < 1) g_occ_p2g = 1;
@@ -1843,6 +1962,58 @@ void launch_step(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev
     k_sur_finish<<<sms * 8, 128, 0, s>>>(P, B); mark();
   }
   k_epilogue<<<1, 32, 0, s>>>(P, B); mark();
+}
+
+// ------------------------------------------------------------------------------------------
+// batched scenes: every kernel of the step launched once for all scenes
+// ------------------------------------------------------------------------------------------
+static const char* kBatchKernelNames[15] = {
+    "kb_prologue", "kb_clear", "kb_count", "kb_scan_local", "kb_scan_top", "kb_scan_add", "kb_scatter",
+    "kb_clear_bricks", "kb_p2g", "kb_grid_update", "kb_g2p_musl", "kb_defgrad", "kb_mlp_infer", "kb_sur_finish",
+    "kb_epilogue"};
+int batched_kernels_per_step(bool surrogate) { return surrogate ? 15 : 13; }
+const char* batched_kernel_name(int i, bool surrogate) {
+  if (i < 0 || i >= batched_kernels_per_step(surrogate)) return "";
+  if (!surrogate && i == 12) return kBatchKernelNames[14];
+  return kBatchKernelNames[i];
+}
+void batched_occupancy(int& p2g, int& g2p, int& def) {
+  p2g = g2p = def = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p2g, kb_p2g, kThreads, p2g_smem_bytes());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g2p, kb_g2p_musl, kThreads, g2p_smem_bytes());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&def, kb_defgrad, kThreads, 0);
+  p2g = p2g < 1 ? 1 : p2g;
+  g2p = g2p < 1 ? 1 : g2p;
+  def = def < 1 ? 1 : def;
+}
+int scan_blocks_for(int node_cap) { return (node_cap + 1 + kScanBlock - 1) / kScanBlock; }
+
+// One round (one step of every scene that has not reached its target) on stream s.  Each launch
+// covers all scenes: CTAs are statically partitioned across scenes by the offset tables, and each
+// CTA loops over its scene's work with the scene's CTA count as stride.
+void launch_step_batched(const BatchLaunch& L, cudaStream_t s, cudaEvent_t* ev) {
+  int e = 0;
+  auto mark = [&]() { if (ev) cudaEventRecord(ev[e++], s); };
+  const SceneDev* sd = L.sd;
+  const int ns = L.ns, ft = L.flat_threads;
+  mark();
+  kb_prologue<<<ns, 32, 0, s>>>(sd, L.off_unit, ns); mark();
+  kb_clear<<<L.n_node, ft, 0, s>>>(sd, L.off_node, ns); mark();
+  kb_count<<<L.n_part, ft, 0, s>>>(sd, L.off_part, ns); mark();
+  kb_scan_local<<<L.n_scan, kScanThreads, 0, s>>>(sd, L.off_scan, ns); mark();
+  kb_scan_top<<<ns, kScanThreads, 0, s>>>(sd, L.off_unit, ns); mark();
+  kb_scan_add<<<L.n_scan, kScanThreads, 0, s>>>(sd, L.off_scan, ns); mark();
+  kb_scatter<<<L.n_part, ft, 0, s>>>(sd, L.off_part, ns); mark();
+  kb_clear_bricks<<<L.n_node, ft, 0, s>>>(sd, L.off_node, ns); mark();
+  kb_p2g<<<L.n_p2g, kThreads, p2g_smem_bytes(), s>>>(sd, L.off_p2g, ns); mark();
+  kb_grid_update<<<L.n_node, ft, 0, s>>>(sd, L.off_node, ns); mark();
+  kb_g2p_musl<<<L.n_g2p, kThreads, g2p_smem_bytes(), s>>>(sd, L.off_g2p, ns); mark();
+  kb_defgrad<<<L.n_def, kThreads, 0, s>>>(sd, L.off_def, ns); mark();
+  if (L.surrogate) {
+    mlp_infer_batched(sd, L.off_sur, ns, L.n_sur, s); mark();
+    kb_sur_finish<<<L.n_sur, 128, 0, s>>>(sd, L.off_sur, ns); mark();
+  }
+  kb_epilogue<<<ns, 32, 0, s>>>(sd, L.off_unit, ns); mark();
 }
 
 void launch_upload(const Params& P, const float* x, const float* lat, const float* v, float* pbuf, uint32_t* meta,

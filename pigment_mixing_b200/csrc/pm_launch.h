@@ -22,4 +22,28 @@ void launch_upload(const Params& P, const float* x, const float* lat, const floa
                    cudaStream_t s);
 void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, double* acc, cudaStream_t s);
 
+// Batched scenes: the SceneDev table and, per kernel class, device tables of CTA offsets
+// (ns + 1 entries; scene s owns CTAs [off[s], off[s+1])) with their totals.
+struct BatchLaunch {
+  const SceneDev* sd = nullptr;
+  int ns = 0;
+  const int* off_unit = nullptr;  // one CTA per scene (prologue, scan_top, epilogue)
+  const int* off_part = nullptr;  // particle-parallel flat kernels (count, scatter)
+  const int* off_node = nullptr;  // node-parallel flat kernels (clear, clear_bricks, grid_update)
+  const int* off_scan = nullptr;  // scan blocks of each scene's cell array
+  const int* off_p2g = nullptr;
+  const int* off_g2p = nullptr;
+  const int* off_def = nullptr;
+  const int* off_sur = nullptr;   // surrogate inference and finish
+  int n_part = 0, n_node = 0, n_scan = 0, n_p2g = 0, n_g2p = 0, n_def = 0, n_sur = 0;
+  int flat_threads = 256;         // block size of the flat kernels
+  bool surrogate = false;         // some scene runs the learned return map
+};
+void launch_step_batched(const BatchLaunch& L, cudaStream_t s, cudaEvent_t* ev = nullptr);
+int batched_kernels_per_step(bool surrogate);
+const char* batched_kernel_name(int i, bool surrogate);
+void batched_occupancy(int& p2g, int& g2p, int& def);
+int scan_blocks_for(int node_cap);
+void mlp_infer_batched(const SceneDev* sd, const int* off, int ns, int ctas, cudaStream_t s);
+
 }  // namespace pm

@@ -20,6 +20,8 @@
 #include <string>
 #include <vector>
 
+#include "pm_internal.cuh"
+#include "pm_launch.h"
 #include "pm_mlp.h"
 
 namespace pm {
@@ -259,11 +261,10 @@ __host__ __device__ constexpr size_t mlp_weights_smem() {
 size_t mlp_stage_bytes() { return mlp_weights_smem(); }
 size_t mlp_infer_smem_bytes() { return mlp_weights_smem() + kMlpWarps * (256 * 2 + 128 * 4); }
 
-__global__ void __launch_bounds__(kMlpThreads) k_mlp_infer(MlpDev gw, const float* X, float* Y, int n,
-                                                           const uint32_t* n_dev) {
+__device__ __forceinline__ void d_mlp_infer(const MlpDev& gw, const float* X, float* Y, int n, const int blk_,
+                                            const int nblk_) {
   extern __shared__ __align__(16) unsigned char smem[];
   MlpDev w = mlp_stage(gw, smem);
-  if (n_dev) n = (int)*n_dev;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smem + mlp_weights_smem()) + warp * 256;
   float* ys = reinterpret_cast<float*>(smem + mlp_weights_smem() + kMlpWarps * 256 * 2) + warp * 128;
@@ -271,8 +272,8 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_infer(MlpDev gw, const floa
   const float* sd = w.stats + 10;
   const float* omean = w.stats + 20;
   const float* osd = w.stats + 26;
-  const int warps = gridDim.x * kMlpWarps;
-  for (int r0 = (blockIdx.x * kMlpWarps + warp) * 16; r0 < n; r0 += warps * 16) {
+  const int warps = nblk_ * kMlpWarps;
+  for (int r0 = (blk_ * kMlpWarps + warp) * 16; r0 < n; r0 += warps * 16) {
     for (int e = lane; e < 256; e += 32) {
       const int r = e >> 4, k = e & 15;
       float v = 0.f;
@@ -288,6 +289,24 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_infer(MlpDev gw, const floa
     }
     __syncwarp();
   }
+}
+
+__global__ void __launch_bounds__(kMlpThreads) k_mlp_infer(MlpDev gw, const float* X, float* Y, int n,
+                                                           const uint32_t* n_dev) {
+  if (n_dev) n = (int)*n_dev;
+  d_mlp_infer(gw, X, Y, n, blockIdx.x, gridDim.x);
+}
+
+// Batched form: scene s infers its own queue (row count from its control block).
+__global__ void __launch_bounds__(kMlpThreads) kb_mlp_infer(const SceneDev* __restrict__ sd, const int* __restrict__ off,
+                                                            int ns) {
+  int s_, blk_, nblk_;
+  batch_slot(off, ns, s_, blk_, nblk_);
+  const SceneDev& d = sd[s_];
+  const Bufs& B = d.B[scene_parity(d)];
+  const Ctrl* c = B.ctrl;
+  if (d.P.return_map != 1 || c->halt || c->idle) return;
+  d_mlp_infer(B.mlp, B.qx, B.qy, (int)c->q_n, blk_, nblk_);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -474,7 +493,14 @@ cudaError_t mlp_upload(const float* params, MlpDev& dev, void** storage) {
 }
 
 cudaError_t mlp_init() {
-  return cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_infer_smem_bytes());
+  cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)mlp_infer_smem_bytes());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kb_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_infer_smem_bytes());
+}
+
+void mlp_infer_batched(const SceneDev* sd, const int* off, int ns, int ctas, cudaStream_t s) {
+  kb_mlp_infer<<<ctas, kMlpThreads, mlp_infer_smem_bytes(), s>>>(sd, off, ns);
 }
 
 cudaError_t mlp_infer(const MlpDev& dev, const float* dX, float* dY, int n, const uint32_t* n_dev, int max_rows,

@@ -23,6 +23,10 @@ MIXBOX_LATENTS = {
                          0.003439664840698242, -0.0034313425421714783, 0.0016628801822662354],
     (0.05, 0.45, 0.25): [0.5207844376564026, 0.42559564113616943, 0.0, 0.05361992120742798,
                          -0.03620488569140434, 0.015082001686096191, 0.0036397576332092285],
+    (0.95, 0.95, 0.93): [0.02470589615404606, 0.02636185847222805, 0.01235294807702303, 0.9365792870521545,
+                         0.0021063685417175293, 0.00013774633407592773, -0.0014260411262512207],
+    (0.45, 0.25, 0.05): [0.26009073853492737, 0.280588299036026, 0.45912498235702515, 0.00019598007202148438,
+                         -0.0287514328956604, 0.02641358971595764, -0.08001551032066345],
 }
 
 RGB_SEEDS = list(MIXBOX_LATENTS)
@@ -125,6 +129,43 @@ def four_block_scene(dx: float, block_cells=(64, 64, 64), seed: int = 0, steps: 
 def config3(seed: int = 0) -> dict:
     """384^3 grid, dx = 1/384, four 64^3-cell blocks of four pigments: 8,388,608 particles."""
     return four_block_scene(1.0 / 384, (64, 64, 64), seed, 2000)
+
+
+def palette_scene(n_particles: int, grid_res: int, pair=(0, 1), yield_pa: float = 100.0, seed: int = 0,
+                  steps: int = 500) -> dict:
+    """One palette scene of the batched workload: the two-block recipe at dx = 1/grid_res with
+    blocks of (2c, 2c, c) cells, c chosen so that 64 c^3 is close to n_particles (and the blocks
+    fit the domain), pigments RGB_SEEDS[pair[0]] and RGB_SEEDS[pair[1]], and von Mises /
+    Herschel-Bulkley paint of the given yield stress (consistency 10 Pa s^0.6 kept)."""
+    c = max(2, int(round((n_particles / 64.0) ** (1.0 / 3.0))))
+    c = min(c, grid_res // 5)
+    sc = two_block_scene(1.0 / grid_res, (2 * c, 2 * c, c), seed, steps)
+    half = len(sc["x"]) // 2
+    sc["latent"] = np.concatenate([np.tile(MIXBOX_LATENTS[RGB_SEEDS[pair[0]]], (half, 1)),
+                                   np.tile(MIXBOX_LATENTS[RGB_SEEDS[pair[1]]], (len(sc["x"]) - half, 1))]
+                                  ).astype(np.float32)
+    sc["params"].update(q_max=float(yield_pa), q_min=float(yield_pa),
+                        perzyna_visc=(10.0 / float(yield_pa)) ** (1.0 / 0.6))
+    sc["name"] = f"palette_{grid_res}_{len(sc['x'])}"
+    return sc
+
+
+def batch_scenes(n: int = 64, seed: int = 0, min_particles: int = 20000, max_particles: int = 400000,
+                 min_grid: int = 64, max_grid: int = 160, steps: int = 500) -> list:
+    """The batched workload: n independent palette scenes, particle counts log-uniform in
+    [min_particles, max_particles], grids min_grid^3 .. max_grid^3 (at least large enough for the
+    blocks), a random pigment pair of the six RGB seeds, yield stress uniform in [50, 200] Pa and a
+    random 3-segment knife path per scene, all from one seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        npart = int(np.exp(rng.uniform(np.log(min_particles), np.log(max_particles))))
+        c = max(2, int(round((npart / 64.0) ** (1.0 / 3.0))))
+        g = int(rng.integers(max(min_grid, 5 * c), max(max_grid, 5 * c) + 1))
+        pair = tuple(int(v) for v in rng.choice(len(RGB_SEEDS), size=2, replace=False))
+        y = float(rng.uniform(50.0, 200.0))
+        out.append(palette_scene(npart, g, pair, y, seed=int(rng.integers(1 << 30)), steps=steps))
+    return out
 
 
 def apply(scene: dict, sim) -> None:

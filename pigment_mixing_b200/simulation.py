@@ -78,6 +78,17 @@ class Simulation:
             return out.value
         raise AttributeError(name)
 
+    def param(self, name: str) -> float:
+        """Any scalar of pm_get_param by name (e.g. "step", which the step() method shadows)."""
+        out = C.c_double()
+        call("pm_get_param", self._h, name.encode(), C.byref(out))
+        return out.value
+
+    @property
+    def steps_done(self) -> int:
+        """Steps completed so far (the control block's step counter)."""
+        return int(self.param("step"))
+
     def __setattr__(self, name, value):
         if name.startswith("_"):
             object.__setattr__(self, name, value)
@@ -267,3 +278,75 @@ class Simulation:
         call("pm_get_grid", self._h, _dp(origin), dims.ctypes.data_as(C.POINTER(C.c_uint32)), _fp(out["mass"]),
              _fp(out["v_update"]), _fp(out["v_musl"]), _fp(out["flip"]), _fp(out["latent"]), _fp(out["shear"]))
         return out
+
+
+class Batch:
+    """Independent prepared scenes stepped together on one GPU (``pm_batch_*``): every kernel of
+    the step is launched once for all scenes, one round is a CUDA graph.  The batch references the
+    simulations; close it before them."""
+
+    def __init__(self, sims):
+        self._sims = list(sims)
+        arr = (C.c_void_p * len(self._sims))(*[s._h.value for s in self._sims])
+        h = C.c_void_p()
+        call("pm_batch_create", arr, len(self._sims), C.byref(h))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            call("pm_batch_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def scenes(self):
+        return list(self._sims)
+
+    def step(self, nsteps: int) -> None:
+        """Advance every scene by nsteps steps."""
+        call("pm_batch_step", self._h, int(nsteps))
+
+    def tuning(self) -> dict:
+        from ._lib import BatchTuning
+        t = BatchTuning()
+        call("pm_batch_get_tuning", self._h, C.byref(t))
+        return t.as_dict()
+
+    def setTuning(self, **kw) -> None:
+        from ._lib import BatchTuning
+        t = BatchTuning()
+        call("pm_batch_get_tuning", self._h, C.byref(t))
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        call("pm_batch_set_tuning", self._h, C.byref(t))
+
+    def autotune(self, trial_rounds: int = 4):
+        """Search the launch shapes (advances the scenes); returns (tuning, ms per round)."""
+        from ._lib import BatchTuning
+        t = BatchTuning()
+        ms = C.c_float()
+        call("pm_batch_autotune", self._h, int(trial_rounds), C.byref(t), C.byref(ms))
+        return t.as_dict(), float(ms.value)
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        call("pm_batch_get_stream", self._h, C.byref(p))
+        return p.value or 0
+
+    @property
+    def kernels_per_round(self) -> int:
+        from ._lib import lib
+        return int(lib().pm_batch_kernels_per_round(self._h))
+
+    def profile(self, rounds: int) -> dict:
+        """Mean CUDA-event duration (ms) of every batched kernel over `rounds` rounds."""
+        from ._lib import lib
+        k = self.kernels_per_round
+        ms = np.zeros(k, np.float32)
+        call("pm_batch_profile", self._h, int(rounds), _fp(ms), k)
+        return {lib().pm_batch_kernel_name(self._h, i).decode(): float(ms[i]) for i in range(k)}
