@@ -129,14 +129,13 @@ struct Params {
 };
 
 // One particle waiting for the surrogate (the state the return map needs to finish).
-struct SurQ {
-  double U[9], V[9];
-  double h[3], hd[3];     // clamped principal log strains, unit deviatoric direction
-  double q_trial, q_y;
+struct __align__(16) SurQ {
+  float U[9], V[9];       // SVD factors of the trial elastic F (rounded from FP64)
+  float h[3], hd[3];      // clamped principal log strains, unit deviatoric direction
+  float q_trial, q_y;
   float epd;
   uint32_t i;             // particle slot (sorted order)
   uint32_t vm;            // 1 VMVisc, 0 DPVisc
-  uint32_t pad;
 };
 
 struct Ctrl {

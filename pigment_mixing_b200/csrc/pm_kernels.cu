@@ -554,26 +554,65 @@ __global__ void kb_scatter(const SceneDev* __restrict__ sd, const int* __restric
 // P2G: warp per cell, lane per stencil node, shared 6x6x6 tile per brick
 // ------------------------------------------------------------------------------------------
 constexpr int kThreads = 128;  // threads per CTA of the brick kernels
+// Minimum resident CTAs per SM the register allocation of G2P+MUSL and the deformation update
+// is sized for (launch bounds): more CTAs hide more latency, fewer leave registers for the
+// FP64 SVD.
+#ifndef PM_DEFGRAD_MINB
+#define PM_DEFGRAD_MINB 5
+#endif
+#ifndef PM_G2P_MINB
+#define PM_G2P_MINB 6
+#endif
 constexpr int kWarps = kThreads / 32;
 constexpr int kP2GCh = 15;
 
-// Per-particle data staged by a warp for its node-parallel scatter: the values every lane reads
-// are grouped into float4s (one 128-bit broadcast load each), the per-axis weights follow.
+// Scatter tiles (P2G channels, MUSL channels) are stored with strides (kSX, kSY, 1) instead of
+// (36, 6, 1): the 27 offsets a*kSX + b*kSY + c (a, b, c in 0..2) of one stencil are then distinct
+// modulo 32, so the 27 lanes of a stencil scatter hit 27 different shared-memory banks.
+constexpr int kSX = 43, kSY = 7;
+// floats per channel of a padded scatter tile (6 * kSX rounded up to 4 floats, so that the staged
+// particle records after the 15 P2G channels stay 16-byte aligned)
+constexpr int kTileStride = (6 * kSX + 3) / 4 * 4;
+static_assert((15 * kTileStride * 4) % 16 == 0 && 5 * kSX + 5 * kSY + 5 < kTileStride, "scatter tile layout");
+__device__ __forceinline__ int tile_pad(int tn) {  // logical node (x*36 + y*6 + z) -> padded offset
+  return (tn / 36) * kSX + ((tn / 6) % 6) * kSY + tn % 6;
+}
+
+
+// Per-particle data staged by a warp for its node-parallel scatter: the values every lane reads,
+// grouped into float4s (one 128-bit broadcast load each).  The B-spline weights are not staged:
+// each lane evaluates the weight of its own stencil node from the particle's position inside its
+// base cell (see StencilPoly).
 struct __align__(16) StageP2G {
-  float4 a;   // q0 q1 q2 diff           (q = v - D B r)
-  float4 c0;  // C0x C0y C0z C1x         (C = D dx B, columns)
+  float4 f;   // fx fy fz diff            (f = (x - x_base) / dx, in [0.5, 1.5))
+  float4 a;   // q0 q1 q2 lat0            (q = v - D B r)
+  float4 c0;  // C0x C0y C0z C1x          (C = D dx B, columns)
   float4 c1;  // C1y C1z C2x C2y
   float4 c2;  // C2z tau_xx tau_yy tau_zz
-  float4 t;   // tau_xy tau_xz tau_yz lat0
-  float4 l0;  // lat1 lat2 lat3 lat4
-  float4 l1;  // lat5 lat6 - -
-  float N[9];   // Nx[3], Ny[3], Nz[3]
-  float dN[9];  // derivatives times inv_dx
-  float pad[2];
+  float4 t;   // tau_xy tau_xz tau_yz lat1
+  float4 l0;  // lat2 lat3 lat4 lat5
+  float4 l1;  // lat6 - - -
 };
-static_assert(sizeof(StageP2G) == 48 * 4, "stage size");
+static_assert(sizeof(StageP2G) == 32 * 4, "stage size");
 
-size_t p2g_smem_bytes() { return sizeof(float) * kP2GCh * kTileNodes + sizeof(StageP2G) * kThreads; }
+// The quadratic B-spline (tools.hpp:153-177) of stencil node k in {0, 1, 2} as a polynomial of the
+// position f in [0.5, 1.5) inside the base cell: N0 = (1.5 - f)^2 / 2, N1 = 3/4 - (f - 1)^2,
+// N2 = (f - 1/2)^2 / 2, and dN/dx = (f - 1.5, 2 - 2f, f - 0.5) / dx.  A lane keeps the
+// coefficients of its node on each axis, so a weight costs three FMAs.
+struct StencilPoly {
+  float n0, n1, n2, d0, d1;  // N = n0 + n1 f + n2 f^2, dN = d0 + d1 f (times 1/dx)
+  __device__ __forceinline__ StencilPoly(int k, float inv_dx) {
+    n0 = k == 0 ? 1.125f : (k == 1 ? -0.25f : 0.125f);
+    n1 = k == 0 ? -1.5f : (k == 1 ? 2.f : -0.5f);
+    n2 = k == 1 ? -1.f : 0.5f;
+    d0 = (k == 0 ? -1.5f : (k == 1 ? 2.f : -0.5f)) * inv_dx;
+    d1 = (k == 1 ? -2.f : 1.f) * inv_dx;
+  }
+  __device__ __forceinline__ float N(float f) const { return fmaf(fmaf(n2, f, n1), f, n0); }
+  __device__ __forceinline__ float dN(float f) const { return fmaf(d1, f, d0); }
+};
+
+size_t p2g_smem_bytes() { return sizeof(float) * kP2GCh * kTileStride + sizeof(StageP2G) * kThreads; }
 
 
 __device__ __forceinline__ int tile_to_node(int tn, int bx, int by, int bz, const Ctrl* c) {
@@ -601,7 +640,7 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
   if (c->halt || c->idle) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* tile = reinterpret_cast<float*>(smem_raw);                       // [kP2GCh][216]
-  StageP2G* stw = reinterpret_cast<StageP2G*>(tile + kP2GCh * kTileNodes);  // [kWarps][32]
+  StageP2G* stw = reinterpret_cast<StageP2G*>(tile + kP2GCh * kTileStride);  // [kWarps][32]
   const int S = P.np_stride;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   StageP2G* st = stw + warp * 32;
@@ -609,13 +648,14 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
   const float fa = (float)la, fb = (float)lb, fc = (float)lc;
   const float D = P.apicD, dx = P.dx;
   const bool apic = P.flip_ratio < 0.f;
+  const StencilPoly px(la, P.inv_dx), py(lb, P.inv_dx), pz(lc, P.inv_dx);
   const int nbr = c->n_bricks;
   for (int b = blk_; b < nbr; b += nblk_) {
     const uint32_t ps = B.cell[(size_t)b * kBrickNodes], pe = B.cell[(size_t)(b + 1) * kBrickNodes];
     if (ps == pe) continue;
     int bx, by, bz;
     brick_coords(b, c, bx, by, bz);
-    for (int i = threadIdx.x; i < kP2GCh * kTileNodes; i += kThreads) tile[i] = 0.f;
+    for (int i = threadIdx.x; i < kP2GCh * kTileStride; i += kThreads) tile[i] = 0.f;
     __syncthreads();
     for (uint32_t c0 = ps + 32u * warp; c0 < pe; c0 += 32u * kWarps) {
       const int n = (int)min(32u, pe - c0);
@@ -629,8 +669,6 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
         for (int d = 0; d < 3; ++d) {
           aw[d] = axis_weights(B.pin[(F_X + d) * S + o], P.anchor[d], dx, P.inv_dx);
           r[d] = aw[d].r;
-#pragma unroll
-          for (int k = 0; k < 3; ++k) { sp.N[3 * d + k] = aw[d].N[k]; sp.dN[3 * d + k] = aw[d].dN[k]; }
         }
         cl = local_cell(aw, c, bx, by, bz);
         float v[3], Bm[9], q[3], C[9];
@@ -649,13 +687,14 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
         for (int k = 0; k < 6; ++k) tau[k] = B.pin[(F_TAU + k) * S + o];
 #pragma unroll
         for (int k = 0; k < 7; ++k) lat[k] = B.pin[(F_LAT + k) * S + o];
-        sp.a = make_float4(q[0], q[1], q[2], B.pin[F_DIFF * S + o]);
+        sp.f = make_float4(r[0] * P.inv_dx, r[1] * P.inv_dx, r[2] * P.inv_dx, B.pin[F_DIFF * S + o]);
+        sp.a = make_float4(q[0], q[1], q[2], lat[0]);
         sp.c0 = make_float4(C[0], C[1], C[2], C[3]);
         sp.c1 = make_float4(C[4], C[5], C[6], C[7]);
         sp.c2 = make_float4(C[8], tau[0], tau[1], tau[2]);
-        sp.t = make_float4(tau[3], tau[4], tau[5], lat[0]);
-        sp.l0 = make_float4(lat[1], lat[2], lat[3], lat[4]);
-        sp.l1 = make_float4(lat[5], lat[6], 0.f, 0.f);
+        sp.t = make_float4(tau[3], tau[4], tau[5], lat[1]);
+        sp.l0 = make_float4(lat[2], lat[3], lat[4], lat[5]);
+        sp.l1 = make_float4(lat[6], 0.f, 0.f, 0.f);
       }
       // runs of equal cells among the warp's particles
       const int prev = __shfl_up_sync(0xffffffffu, cl, 1);
@@ -672,12 +711,12 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
           for (int k = 0; k < kP2GCh; ++k) acc[k] = 0.f;
           for (int q = s0; q < s1; ++q) {
             const StageP2G& sp = st[q];
-            const float nx = sp.N[la], ny = sp.N[3 + lb], nz = sp.N[6 + lc];
+            const float4 Fr = sp.f, A = sp.a, C0 = sp.c0, C1 = sp.c1, C2 = sp.c2, T = sp.t, L0 = sp.l0, L1 = sp.l1;
+            const float nx = px.N(Fr.x), ny = py.N(Fr.y), nz = pz.N(Fr.z);
             const float nyz = ny * nz;
             const float w = nx * nyz;
-            const float gx = sp.dN[la] * nyz, gy = nx * sp.dN[3 + lb] * nz, gz = nx * ny * sp.dN[6 + lc];
+            const float gx = px.dN(Fr.x) * nyz, gy = nx * py.dN(Fr.y) * nz, gz = nx * ny * pz.dN(Fr.z);
             const float wm = w > 1e-25f ? w : 0.f;  // p2g.cpp:39
-            const float4 A = sp.a, C0 = sp.c0, C1 = sp.c1, C2 = sp.c2, T = sp.t, L0 = sp.l0, L1 = sp.l1;
             acc[0] += wm;
             acc[1] += wm * (A.x + fa * C0.x + fb * C0.w + fc * C1.z);
             acc[2] += wm * (A.y + fa * C0.y + fb * C1.x + fc * C1.w);
@@ -685,35 +724,35 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
             acc[4] += C2.y * gx + T.x * gy + T.y * gz;
             acc[5] += T.x * gx + C2.z * gy + T.z * gz;
             acc[6] += T.y * gx + T.z * gy + C2.w * gz;
-            acc[7] += wm * T.w;
-            acc[8] += wm * L0.x;
-            acc[9] += wm * L0.y;
-            acc[10] += wm * L0.z;
-            acc[11] += wm * L0.w;
-            acc[12] += wm * L1.x;
-            acc[13] += wm * L1.y;
-            acc[14] += wm * A.w;
+            acc[7] += wm * A.w;
+            acc[8] += wm * T.w;
+            acc[9] += wm * L0.x;
+            acc[10] += wm * L0.y;
+            acc[11] += wm * L0.z;
+            acc[12] += wm * L0.w;
+            acc[13] += wm * L1.x;
+            acc[14] += wm * Fr.w;
           }
-          const int tn = (((cell >> 4) + la) * kTile + (((cell >> 2) & 3) + lb)) * kTile + ((cell & 3) + lc);
+          const int tp = ((cell >> 4) + la) * kSX + (((cell >> 2) & 3) + lb) * kSY + ((cell & 3) + lc);
 #pragma unroll
           for (int k = 0; k < kP2GCh; ++k)
-            if (acc[k] != 0.f) atomicAdd(&tile[k * kTileNodes + tn], acc[k]);
+            if (acc[k] != 0.f) atomicAdd(&tile[k * kTileStride + tp], acc[k]);
         }
       }
       __syncwarp();
     }
     __syncthreads();
     for (int tn = threadIdx.x; tn < kTileNodes; tn += kThreads) {
-      const float m = tile[tn];
+      const float* t = tile + tile_pad(tn);
+      const float m = t[0];
       if (m == 0.f) continue;
       const int node = tile_to_node(tn, bx, by, bz, c);
       if (node < 0) continue;
       float4* rec = B.grid + (size_t)node * 4;
-      const float* t = tile + tn;
-      red_add_v4(rec + 0, m, t[1 * kTileNodes], t[2 * kTileNodes], t[3 * kTileNodes]);
-      red_add_v4(rec + 1, t[4 * kTileNodes], t[5 * kTileNodes], t[6 * kTileNodes], t[7 * kTileNodes]);
-      red_add_v4(rec + 2, t[8 * kTileNodes], t[9 * kTileNodes], t[10 * kTileNodes], t[11 * kTileNodes]);
-      red_add_v4(rec + 3, t[12 * kTileNodes], t[13 * kTileNodes], t[14 * kTileNodes], 0.f);
+      red_add_v4(rec + 0, m, t[1 * kTileStride], t[2 * kTileStride], t[3 * kTileStride]);
+      red_add_v4(rec + 1, t[4 * kTileStride], t[5 * kTileStride], t[6 * kTileStride], t[7 * kTileStride]);
+      red_add_v4(rec + 2, t[8 * kTileStride], t[9 * kTileStride], t[10 * kTileStride], t[11 * kTileStride]);
+      red_add_v4(rec + 3, t[12 * kTileStride], t[13 * kTileStride], t[14 * kTileStride], 0.f);
     }
     __syncthreads();
   }
@@ -966,17 +1005,15 @@ __global__ void kb_grid_update(const SceneDev* __restrict__ sd, const int* __res
 // G2P + mixing + MUSL (velocity update and re-scatter)
 // ------------------------------------------------------------------------------------------
 struct __align__(16) StageMUSL {
-  float4 q;    // q0 q1 q2 -   (q = v_new - D B_new r)
+  float4 q;    // q0 q1 q2 fx  (q = v_new - D B_new r; f = position in the base cell, StencilPoly)
   float4 c0;   // C0x C0y C0z C1x
   float4 c1;   // C1y C1z C2x C2y
-  float4 c2;   // C2z - - -
-  float N[9];
-  float pad[3];
+  float4 c2;   // C2z fy fz -
 };
-static_assert(sizeof(StageMUSL) == 28 * 4, "stage size");
+static_assert(sizeof(StageMUSL) == 16 * 4, "stage size");
 
 size_t g2p_smem_bytes() {
-  return sizeof(float4) * 4 * kTileNodes + sizeof(float) * 4 * kTileNodes + sizeof(StageMUSL) * kThreads;
+  return sizeof(float4) * 4 * kTileNodes + sizeof(float) * 4 * kTileStride + sizeof(StageMUSL) * kThreads;
 }
 
 __device__ __forceinline__ float smooth_step(float e0, float e1, float x) {  // g2p.cpp:7-10
@@ -994,13 +1031,14 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
   if (c->halt || c->idle) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* tile = reinterpret_cast<float4*>(smem_raw);              // [216][4]
-  float* mtile = reinterpret_cast<float*>(tile + 4 * kTileNodes);  // [4][216]
-  StageMUSL* stw = reinterpret_cast<StageMUSL*>(mtile + 4 * kTileNodes);
+  float* mtile = reinterpret_cast<float*>(tile + 4 * kTileNodes);  // [4][kTileStride], padded layout
+  StageMUSL* stw = reinterpret_cast<StageMUSL*>(mtile + 4 * kTileStride);
   const int S = P.np_stride;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   StageMUSL* st = stw + warp * 32;
   const int la = lane / 9, lb = (lane / 3) % 3, lc = lane % 3;
   const float fa = (float)la, fb = (float)lb, fcc = (float)lc;
+  const StencilPoly px(la, P.inv_dx), py(lb, P.inv_dx), pz(lc, P.inv_dx);
   const float D = P.apicD, dx = P.dx;
   const float fr = P.flip_ratio;
   const bool apic = fr < 0.f, use_flip = fr >= -1.f, musl = P.use_musl != 0;
@@ -1026,7 +1064,7 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
       const int node = tile_to_node(i >> 2, bx, by, bz, c);
       tile[i] = node >= 0 ? B.grid[(size_t)node * 4 + (i & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    for (int i = threadIdx.x; i < 4 * kTileNodes; i += kThreads) mtile[i] = 0.f;
+    for (int i = threadIdx.x; i < 4 * kTileStride; i += kThreads) mtile[i] = 0.f;
     __syncthreads();
     for (uint32_t c0 = ps + 32u * warp; c0 < pe; c0 += 32u * kWarps) {
       const int n = (int)min(32u, pe - c0);
@@ -1123,10 +1161,6 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
         po[F_DIFF * S + i] = diff;
         if (musl) {
           StageMUSL& sp = st[lane];
-#pragma unroll
-          for (int d = 0; d < 3; ++d)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) sp.N[3 * d + k] = aw[d].N[k];
           const float r3[3] = {aw[0].r, aw[1].r, aw[2].r};
           float q[3], C[9];
 #pragma unroll
@@ -1136,10 +1170,10 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
           for (int k = 0; k < 3; ++k)
 #pragma unroll
             for (int qq = 0; qq < 3; ++qq) C[3 * k + qq] = D * dx * Bp[3 * qq + k];
-          sp.q = make_float4(q[0], q[1], q[2], 0.f);
+          sp.q = make_float4(q[0], q[1], q[2], r3[0] * P.inv_dx);
           sp.c0 = make_float4(C[0], C[1], C[2], C[3]);
           sp.c1 = make_float4(C[4], C[5], C[6], C[7]);
-          sp.c2 = make_float4(C[8], 0.f, 0.f, 0.f);
+          sp.c2 = make_float4(C[8], r3[1] * P.inv_dx, r3[2] * P.inv_dx, 0.f);
         }
       }
       if (musl) {
@@ -1155,18 +1189,17 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
             for (int q = s0; q < s1; ++q) {
               const StageMUSL& sp = st[q];
-              const float w = sp.N[la] * (sp.N[3 + lb] * sp.N[6 + lc]);
-              const float wm = w > 1e-25f ? w : 0.f;  // musl.cpp:188
               const float4 Q = sp.q, C0 = sp.c0, C1 = sp.c1, C2 = sp.c2;
+              const float w = px.N(Q.w) * (py.N(C2.y) * pz.N(C2.z));
+              const float wm = w > 1e-25f ? w : 0.f;  // musl.cpp:188
               acc[0] += wm * (Q.x + fa * C0.x + fb * C0.w + fcc * C1.z);
               acc[1] += wm * (Q.y + fa * C0.y + fb * C1.x + fcc * C1.w);
               acc[2] += wm * (Q.z + fa * C0.z + fb * C1.y + fcc * C2.x);
               acc[3] += wm;
             }
-            const int tn = (((cell >> 4) + la) * kTile + (((cell >> 2) & 3) + lb)) * kTile + ((cell & 3) + lc);
+            const int tp = ((cell >> 4) + la) * kSX + (((cell >> 2) & 3) + lb) * kSY + ((cell & 3) + lc);
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-              if (acc[k] != 0.f) atomicAdd(&mtile[k * kTileNodes + tn], acc[k]);
+            for (int k = 0; k < 4; ++k) atomicAdd(&mtile[k * kTileStride + tp], acc[k]);
           }
         }
         __syncwarp();
@@ -1175,18 +1208,19 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
     __syncthreads();
     if (musl) {
       for (int tn = threadIdx.x; tn < kTileNodes; tn += kThreads) {
-        const float w = mtile[3 * kTileNodes + tn];
+        const float* t = mtile + tile_pad(tn);
+        const float w = t[3 * kTileStride];
         if (w == 0.f) continue;
         const int node = tile_to_node(tn, bx, by, bz, c);
         if (node < 0) continue;
-        red_add_v4(B.gmusl + node, mtile[tn], mtile[kTileNodes + tn], mtile[2 * kTileNodes + tn], w);
+        red_add_v4(B.gmusl + node, t[0], t[kTileStride], t[2 * kTileStride], w);
       }
     }
     __syncthreads();
   }
 }
-__global__ void __launch_bounds__(kThreads, 5) k_g2p_musl(Params P, Bufs B) { d_g2p_musl(P, B, blockIdx.x, gridDim.x); }
-__global__ void __launch_bounds__(kThreads, 5) kb_g2p_musl(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+__global__ void __launch_bounds__(kThreads, PM_G2P_MINB) k_g2p_musl(Params P, Bufs B) { d_g2p_musl(P, B, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kThreads, PM_G2P_MINB) kb_g2p_musl(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
   int s_, blk_, nblk_;
   batch_slot(off, ns, s_, blk_, nblk_);
   const SceneDev& d_ = sd[s_];
@@ -1364,7 +1398,7 @@ __device__ void svd3_warm(const double A[9], double U[9], double s[3], double V[
 // deformation update + return map + position update + stress cache + reductions
 // ------------------------------------------------------------------------------------------
 struct ReturnMapOut {
-  double h[3];       // final principal log strains
+  float h[3];        // final principal log strains
   bool changed;      // F replaced by U exp(h) V^T
   bool to_rotation;  // capped VM branch: F = U V^T
   bool queued;       // surrogate mode: the consistency solve is left to the surrogate pass
@@ -1395,46 +1429,76 @@ __device__ double perzyna_newton(const Params& P, bool vm, double q_trial, doubl
   return dg;
 }
 
+// The same Perzyna Newton for VMVisc in FP32 (plasticity.cpp:194-229).  The stop test is
+// |r| < max(1e-2, 1e-6 q_trial): the reference's 1e-2 Pa unless q_trial exceeds 1e4 Pa, where
+// FP32 rounding of q would otherwise keep |r| above 1e-2.
+__device__ float perzyna_newton_vm32(const Params& P, float q_trial, float epd, float dt, float dg, uint32_t& iters,
+                                     uint32_t& err) {
+  const float fmu = (float)P.f_mu_prefac, dpre = (float)P.d_prefac, visc = (float)P.perzyna_visc;
+  const float m = (float)P.perzyna_exp, qmin = (float)P.q_min, dq = (float)(P.q_max - P.q_min), xi = (float)P.xi;
+  const float tol = fmaxf(1e-2f, 1e-6f * q_trial);
+  for (int it = 0; it < 60; ++it) {
+    if (it == 59) err |= E_NEWTON_NOCONV;
+    const float tm = visc * dg + dt;
+    const float tmp = dt / tm;
+    const float tmp1 = exp2f(m * log2f(tmp));  // tmp^m; tmp^(m-1) = tmp1 / tmp
+    const float tmpm1 = tmp1 / tmp;
+    const float soft = xi != 0.f ? expf(-xi * (epd + dg / dpre)) : 1.f;
+    const float res = (q_trial - fmu * dg) * tmp1 - (qmin + dq * soft);
+    if (fabsf(res) < tol) break;
+    const float qyd = -xi / dpre * dq * soft;
+    const float rd = -fmu * tmp1 + (q_trial - fmu * dg) * m * tmpm1 * (-visc * dt) / (tm * tm) - qyd;
+    if (fabsf(rd) < 1e-14f) err |= E_NEWTON_FLAT;
+    dg -= res / rd;
+    if (dg < 0.f) dg = 1e-10f;
+    ++iters;
+  }
+  return dg;
+}
+
 // Surrogate features of a particle on the Newton path: trial log strains, deviatoric strain
 // rate, yield, viscosity, flow index, Young's modulus.
-__device__ __forceinline__ void sur_features(const Params& P, const double h[3], double dt, double q_yield, float f[10]) {
-  const double m = (h[0] + h[1] + h[2]) / 3.0;
-  for (int k = 0; k < 3; ++k) { f[k] = (float)h[k]; f[3 + k] = (float)((h[k] - m) / dt); }
-  f[6] = (float)q_yield;
+__device__ __forceinline__ void sur_features(const Params& P, const float h[3], float dt, float q_yield, float f[10]) {
+  const float m = (h[0] + h[1] + h[2]) / 3.f;
+  for (int k = 0; k < 3; ++k) { f[k] = h[k]; f[3 + k] = (h[k] - m) / dt; }
+  f[6] = q_yield;
   f[7] = (float)P.perzyna_visc;
   f[8] = (float)P.perzyna_exp;
   f[9] = (float)P.E;
 }
 
 // The Newton path of the return map: either queue the particle for the surrogate, or solve
-// (and, when the sample log is on, record features and the projected strains).
-__device__ bool newton_path(const Params& P, const Bufs& B, uint32_t i, bool vm, double dt, const double h[3],
-                            const double hd[3], double q_trial, double q_yield, float epd, const double* U,
-                            const double* V, double& dg, uint32_t& iters, uint32_t& err) {
+// (VMVisc in FP32, DPVisc in FP64) and, when the sample log is on, record features and the
+// projected strains.
+__device__ bool newton_path(const Params& P, const Bufs& B, uint32_t i, bool vm, double dt, const float h[3],
+                            const float hd[3], double q_trial, double q_yield, float epd, const float* U,
+                            const float* V, double& dg, uint32_t& iters, uint32_t& err) {
   if (P.return_map == 1 && P.q_cap > 0) {
     const uint32_t slot = atomicAdd(&B.ctrl->q_n, 1u);
     if (slot < P.q_cap) {
       SurQ& r = B.q[slot];
       for (int k = 0; k < 9; ++k) { r.U[k] = U[k]; r.V[k] = V[k]; }
       for (int k = 0; k < 3; ++k) { r.h[k] = h[k]; r.hd[k] = hd[k]; }
-      r.q_trial = q_trial;
-      r.q_y = q_yield;
+      r.q_trial = (float)q_trial;
+      r.q_y = (float)q_yield;
       r.epd = epd;
       r.i = i;
       r.vm = vm ? 1u : 0u;
       float f[10];
-      sur_features(P, h, dt, q_yield, f);
+      sur_features(P, h, (float)dt, (float)q_yield, f);
       for (int k = 0; k < 10; ++k) B.qx[(size_t)slot * 10 + k] = f[k];
       return true;
     }
     err |= E_CAPACITY;  // queue full: solve here
   }
-  dg = perzyna_newton(P, vm, q_trial, q_yield, (double)epd, dt, 0.01 * (q_trial - q_yield) / P.f_mu_prefac, iters, err);
+  const double guess = 0.01 * (q_trial - q_yield) / P.f_mu_prefac;
+  if (vm) dg = perzyna_newton_vm32(P, (float)q_trial, epd, (float)dt, (float)guess, iters, err);
+  else dg = perzyna_newton(P, false, q_trial, q_yield, (double)epd, dt, guess, iters, err);
   if (P.log_cap > 0 && (P.log_every <= 1 || ((i ^ (B.ctrl->step * 0x9E3779B9u)) * 0x85EBCA6Bu >> 8) % P.log_every == 0)) {
     const uint32_t slot = atomicAdd(&B.ctrl->slog_n, 1u);
     if (slot < P.log_cap) {
       float* o = B.slog + (size_t)slot * 16;
-      sur_features(P, h, dt, q_yield, o);
+      sur_features(P, h, (float)dt, (float)q_yield, o);
       for (int k = 0; k < 3; ++k) {
         const double d = (dg / P.d_prefac) * hd[k];  // h - h_projected
         o[10 + k] = (float)d;
@@ -1445,48 +1509,61 @@ __device__ bool newton_path(const Params& P, const Bufs& B, uint32_t i, bool vm,
   return false;
 }
 
-// plasticity.cpp:163-238 (VMVisc) and :240-340 (DPVisc) in FP64
-__device__ void return_map(const Params& P, const Bufs& B, uint32_t i, double dt, const double sg[3], const double* U,
-                           const double* V, float& epd, float& epv, float& epp, float& dgam, uint32_t& plastic,
+// plasticity.cpp:163-238 (VMVisc, FP32) and :240-340 (DPVisc, FP64: the cone and its apex).
+// sg: singular values of the trial elastic F (FP64 SVD); U, V its factors rounded to FP32.
+__device__ void return_map(const Params& P, const Bufs& B, uint32_t i, double dt, const double sg[3], const float* U,
+                           const float* V, float& epd, float& epv, float& epp, float& dgam, uint32_t& plastic,
                            uint32_t& iters, uint32_t& solves, uint32_t& err, ReturnMapOut& out) {
-  double h[3];
-  for (int k = 0; k < 3; ++k) h[k] = log(fmax(fabs(sg[k]), 1e-4));
-  const double htr = h[0] + h[1] + h[2];
-  double hd[3] = {h[0] - htr / 3.0, h[1] - htr / 3.0, h[2] - htr / 3.0};
-  const double hdn = sqrt(hd[0] * hd[0] + hd[1] * hd[1] + hd[2] * hd[2]);
-  if (hdn > 0) for (int k = 0; k < 3; ++k) hd[k] /= hdn;
   out.changed = false;
   out.to_rotation = false;
   out.queued = false;
-  for (int k = 0; k < 3; ++k) out.h[k] = h[k];
-  const double fmu = P.f_mu_prefac, emu = P.e_mu_prefac, dpre = P.d_prefac;
   if (P.plastic_model == PL_VMVISC) {
-    const double q_trial = emu * hdn;
-    double q_yield = P.q_min + (P.q_max - P.q_min) * exp(-P.xi * (double)epd);
-    const double p_trial = -P.K * htr;
-    if (p_trial < P.p_min * exp(-P.xi * (double)epv)) {
-      const double dg = q_trial / fmu;
+    float h[3];
+    for (int k = 0; k < 3; ++k) h[k] = logf(fmaxf(fabsf((float)sg[k]), 1e-4f));
+    const float htr = h[0] + h[1] + h[2];
+    float hd[3] = {h[0] - htr / 3.f, h[1] - htr / 3.f, h[2] - htr / 3.f};
+    const float hdn = sqrtf(hd[0] * hd[0] + hd[1] * hd[1] + hd[2] * hd[2]);
+    if (hdn > 0.f) for (int k = 0; k < 3; ++k) hd[k] /= hdn;
+    for (int k = 0; k < 3; ++k) out.h[k] = h[k];
+    const float fmu = (float)P.f_mu_prefac, emu = (float)P.e_mu_prefac, dpre = (float)P.d_prefac, K = (float)P.K;
+    const float xi = (float)P.xi;
+    const float q_trial = emu * hdn;
+    const float q_yield = (float)P.q_min + (float)(P.q_max - P.q_min) * expf(-xi * epd);
+    const float p_trial = -K * htr;
+    const float dtf = (float)dt;
+    if (p_trial < (float)P.p_min * expf(-xi * epv)) {
+      const float dg = q_trial / fmu;
       out.to_rotation = true;
       out.changed = true;
-      epv = (float)((double)epv + (-p_trial / P.K));
-      epd = (float)((double)epd + dg / dpre);
-      dgam = (float)(dg / dt);
+      epv += -p_trial / K;
+      epd += dg / dpre;
+      dgam = dg / dtf;
     } else if (q_trial > q_yield) {
       ++plastic;
-      double dg = 0.0;
+      float dg = 0.f;
       if (P.perzyna_exp == 1.0 && P.xi == 0.0) {
-        dg = (q_trial - q_yield) / (fmu + q_yield * P.perzyna_visc / dt);
-        if (dg < 0) err |= E_NEG_DGAMMA;
+        dg = (q_trial - q_yield) / (fmu + q_yield * (float)P.perzyna_visc / dtf);
+        if (dg < 0.f) err |= E_NEG_DGAMMA;
       } else {
         ++solves;
-        if (newton_path(P, B, i, true, dt, h, hd, q_trial, q_yield, epd, U, V, dg, iters, err)) { out.queued = true; return; }
+        double dgd = 0.0;
+        if (newton_path(P, B, i, true, dt, h, hd, q_trial, q_yield, epd, U, V, dgd, iters, err)) { out.queued = true; return; }
+        dg = (float)dgd;
       }
       for (int k = 0; k < 3; ++k) out.h[k] = h[k] - (dg / dpre) * hd[k];
       out.changed = true;
-      epd = (float)((double)epd + dg / dpre);
-      dgam = (float)(dg / dt);
+      epd += dg / dpre;
+      dgam = dg / dtf;
     }
   } else if (P.plastic_model == PL_DPVISC) {
+    double h[3];
+    for (int k = 0; k < 3; ++k) h[k] = log(fmax(fabs(sg[k]), 1e-4));
+    const double htr = h[0] + h[1] + h[2];
+    double hd[3] = {h[0] - htr / 3.0, h[1] - htr / 3.0, h[2] - htr / 3.0};
+    const double hdn = sqrt(hd[0] * hd[0] + hd[1] * hd[1] + hd[2] * hd[2]);
+    if (hdn > 0) for (int k = 0; k < 3; ++k) hd[k] /= hdn;
+    for (int k = 0; k < 3; ++k) out.h[k] = (float)h[k];
+    const double fmu = P.f_mu_prefac, emu = P.e_mu_prefac, dpre = P.d_prefac;
     const double p_trial = -P.K * htr;
     const double q_trial = emu * hdn;
     const double p_tip = -P.q_cohesion / P.M;
@@ -1497,7 +1574,7 @@ __device__ void return_map(const Params& P, const Bufs& B, uint32_t i, double dt
       const double epv_inst = (p_tip - p_trial) / P.K;
       ++plastic;
       const double hh = -p_tip / (P.K * 3.0);
-      for (int k = 0; k < 3; ++k) out.h[k] = hh;
+      for (int k = 0; k < 3; ++k) out.h[k] = (float)hh;
       out.changed = true;
       dgam = (float)(dg / dt);
       epd = (float)((double)epd + dg / dpre);
@@ -1515,9 +1592,11 @@ __device__ void return_map(const Params& P, const Bufs& B, uint32_t i, double dt
         if (dg < 0) err |= E_NEG_DGAMMA;
       } else {
         ++solves;
-        if (newton_path(P, B, i, false, dt, h, hd, q_trial, q_yield, epd, U, V, dg, iters, err)) { out.queued = true; return; }
+        const float hf[3] = {(float)h[0], (float)h[1], (float)h[2]};
+        const float hdf[3] = {(float)hd[0], (float)hd[1], (float)hd[2]};
+        if (newton_path(P, B, i, false, dt, hf, hdf, q_trial, q_yield, epd, U, V, dg, iters, err)) { out.queued = true; return; }
       }
-      for (int k = 0; k < 3; ++k) out.h[k] = h[k] - (dg / dpre) * hd[k];
+      for (int k = 0; k < 3; ++k) out.h[k] = (float)(h[k] - (dg / dpre) * hd[k]);
       out.changed = true;
       epd = (float)((double)epd + dg / dpre);
       dgam = (float)(dg / dt);
@@ -1526,27 +1605,28 @@ __device__ void return_map(const Params& P, const Bufs& B, uint32_t i, double dt
 }
 
 // F = U exp(h) V^T and the Kirchhoff stress tau = U diag(2 mu h + lambda tr h) U^T of the final F
-// (simulation.hpp:287-294 evaluated on the factors the return map already has).
-__device__ __forceinline__ void finish_F_tau(const Params& P, const double* U, const double* V, const double hfin[3],
-                                             bool rebuild, const double* Ft, float Fout[9], float tau[6]) {
+// (simulation.hpp:287-294 evaluated on the factors the return map already has), in FP32.
+__device__ __forceinline__ void finish_F_tau(const Params& P, const float* U, const float* V, const float hfin[3],
+                                             bool rebuild, const float* Ft, float Fout[9], float tau[6]) {
   if (rebuild) {
-    const double e[3] = {exp(hfin[0]), exp(hfin[1]), exp(hfin[2])};
+    const float e[3] = {expf(hfin[0]), expf(hfin[1]), expf(hfin[2])};
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int q = 0; q < 3; ++q)
-        Fout[3 * r + q] = (float)(U[3 * r] * e[0] * V[3 * q] + U[3 * r + 1] * e[1] * V[3 * q + 1] + U[3 * r + 2] * e[2] * V[3 * q + 2]);
+        Fout[3 * r + q] = U[3 * r] * e[0] * V[3 * q] + U[3 * r + 1] * e[1] * V[3 * q + 1] + U[3 * r + 2] * e[2] * V[3 * q + 2];
   } else {
 #pragma unroll
-    for (int k = 0; k < 9; ++k) Fout[k] = (float)Ft[k];
+    for (int k = 0; k < 9; ++k) Fout[k] = Ft[k];
   }
-  const double tr = hfin[0] + hfin[1] + hfin[2];
-  double d[3];
-  for (int k = 0; k < 3; ++k) d[k] = 2.0 * P.mu * hfin[k] + P.lambda * tr;
-  if (!(isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2]))) { d[0] = d[1] = d[2] = 0.0; }
+  const float tr = hfin[0] + hfin[1] + hfin[2];
+  const float mu2 = (float)(2.0 * P.mu), lam = (float)P.lambda;
+  float d[3];
+  for (int k = 0; k < 3; ++k) d[k] = mu2 * hfin[k] + lam * tr;
+  if (!(isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2]))) { d[0] = d[1] = d[2] = 0.f; }
   auto T = [&](int r, int q) { return U[3 * r] * d[0] * U[3 * q] + U[3 * r + 1] * d[1] * U[3 * q + 1] + U[3 * r + 2] * d[2] * U[3 * q + 2]; };
-  tau[0] = (float)T(0, 0); tau[1] = (float)T(1, 1); tau[2] = (float)T(2, 2);
-  tau[3] = (float)T(0, 1); tau[4] = (float)T(0, 2); tau[5] = (float)T(1, 2);
+  tau[0] = T(0, 0); tau[1] = T(1, 1); tau[2] = T(2, 2);
+  tau[3] = T(0, 1); tau[4] = T(0, 2); tau[5] = T(1, 2);
 }
 
 __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
@@ -1620,46 +1700,8 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
 #pragma unroll
             for (int q = 0; q < 3; ++q) L[3 * r + q] += gv[r] * g[q];
         }
-    // F_trial = F + dt L F (FP64)
-    double F[9], Ft[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) F[k] = (double)pi[(F_F + k) * S + o];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        double s = 0.0;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) s += (double)L[3 * r + k] * F[3 * k + q];
-        Ft[3 * r + q] = F[3 * r + q] + dt * s;
-      }
-    float epd = pi[F_EPD * S + o], epv = pi[F_EPV * S + o], epp = pi[F_EPP * S + o], dgam = 0.f;
-    double U[9], V[9], sg[3];
-    svd3_warm(Ft, U, sg, V);
-    double hfin[3];
-    bool changed = false, queued = false;
-    if (P.plastic_model != PL_NONE) {
-      ReturnMapOut rm;
-      return_map(P, B, (uint32_t)i, dt, sg, U, V, epd, epv, epp, dgam, plastic, niters, nsolves, err, rm);
-      changed = rm.changed;
-      queued = rm.queued;
-      if (rm.to_rotation) { hfin[0] = hfin[1] = hfin[2] = 0.0; }
-      else for (int k = 0; k < 3; ++k) hfin[k] = rm.h[k];
-    }
-    if (!changed) for (int k = 0; k < 3; ++k) hfin[k] = log(fabs(sg[k]));
-    if (!queued) {  // queued particles get F, tau, eps_pl_dev and delta_gamma from the surrogate pass
-      float Fout[9], tau[6];
-      finish_F_tau(P, U, V, hfin, changed, Ft, Fout, tau);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = Fout[k];
-#pragma unroll
-      for (int k = 0; k < 6; ++k) po[(F_TAU + k) * S + i] = tau[k];
-      po[F_EPD * S + i] = epd;
-      po[F_DG * S + i] = dgam;
-    }
-    po[F_EPV * S + i] = epv;
-    po[F_EPP * S + i] = epp;
-    // position update (position_update.cpp:6-91)
+    // position update (position_update.cpp:6-91); done before the SVD so that its values are not
+    // live across it
     float pic[3], v[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) { pic[r] = B.pic[r * S + i]; v[r] = po[(F_V + r) * S + i]; }
@@ -1700,6 +1742,54 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
       maxv2 = fmaxf(maxv2, v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
       for (int r = 0; r < 3; ++r) { int k = fkey(xn[r]); mn[r] = min(mn[r], k); mx[r] = max(mx[r], k); }
     }
+    // F_trial = F + dt L F (FP64)
+    double F[9], Ft[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) F[k] = (double)pi[(F_F + k) * S + o];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s += (double)L[3 * r + k] * F[3 * k + q];
+        Ft[3 * r + q] = F[3 * r + q] + dt * s;
+      }
+    float epd = pi[F_EPD * S + o], epv = pi[F_EPV * S + o], epp = pi[F_EPP * S + o], dgam = 0.f;
+    float Ftf[9];  // F_trial as stored when the return map leaves it unchanged
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Ftf[k] = (float)Ft[k];
+    double sg[3];
+    float U[9], V[9];
+    {
+      double Ud[9], Vd[9];
+      svd3_warm(Ft, Ud, sg, Vd);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) { U[k] = (float)Ud[k]; V[k] = (float)Vd[k]; }
+    }
+    float hfin[3];
+    bool changed = false, queued = false;
+    if (P.plastic_model != PL_NONE) {
+      ReturnMapOut rm;
+      return_map(P, B, (uint32_t)i, dt, sg, U, V, epd, epv, epp, dgam, plastic, niters, nsolves, err, rm);
+      changed = rm.changed;
+      queued = rm.queued;
+      if (rm.to_rotation) { hfin[0] = hfin[1] = hfin[2] = 0.f; }
+      else for (int k = 0; k < 3; ++k) hfin[k] = rm.h[k];
+    }
+    if (!changed) for (int k = 0; k < 3; ++k) hfin[k] = logf(fabsf((float)sg[k]));
+    if (!queued) {  // queued particles get F, tau, eps_pl_dev and delta_gamma from the surrogate pass
+      float Fout[9], tau[6];
+      finish_F_tau(P, U, V, hfin, changed, Ftf, Fout, tau);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = Fout[k];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) po[(F_TAU + k) * S + i] = tau[k];
+      po[F_EPD * S + i] = epd;
+      po[F_DG * S + i] = dgam;
+    }
+    po[F_EPV * S + i] = epv;
+    po[F_EPP * S + i] = epp;
   }
   // block reduction, then one set of atomics per block
   __shared__ int red_i[kWarps][8];
@@ -1737,8 +1827,8 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     if (red_u[0][3]) atomicOr(&cw->error_flags, red_u[0][3]);
   }
 }
-__global__ void __launch_bounds__(kThreads, 5) k_defgrad(Params P, Bufs B) { d_defgrad(P, B, blockIdx.x, gridDim.x); }
-__global__ void __launch_bounds__(kThreads, 5) kb_defgrad(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+__global__ void __launch_bounds__(kThreads, PM_DEFGRAD_MINB) k_defgrad(Params P, Bufs B) { d_defgrad(P, B, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kThreads, PM_DEFGRAD_MINB) kb_defgrad(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
   int s_, blk_, nblk_;
   batch_slot(off, ns, s_, blk_, nblk_);
   const SceneDev& d_ = sd[s_];
@@ -1765,20 +1855,24 @@ __device__ __forceinline__ void d_sur_finish(const Params& P, const Bufs& B, con
     double pd = 0.0, pr = 0.0;
     for (int j = 0; j < 3; ++j) { pd += (double)y[j] * r.hd[j]; pr += (double)y[3 + j] * r.hd[j]; }
     double dg = P.d_prefac * 0.5 * (pd + pr * dt);
-    const double dg_max = r.q_trial / P.f_mu_prefac;
+    const double dg_max = (double)r.q_trial / P.f_mu_prefac;
     if (!(dg >= 0.0)) dg = 0.0;
     if (dg > dg_max) dg = dg_max;
     uint32_t it = 0;
     const bool vm = r.vm != 0;
-    double dgf = perzyna_newton(P, vm, r.q_trial, r.q_y, (double)r.epd, dt, dg, it, err);
+    auto solve = [&](double start) -> double {
+      if (vm) return perzyna_newton_vm32(P, r.q_trial, r.epd, (float)dt, (float)start, it, err);
+      return perzyna_newton(P, false, r.q_trial, r.q_y, (double)r.epd, dt, start, it, err);
+    };
+    double dgf = solve(dg);
     if (it == 0) ++accepted;
     else if (P.sur_fallback_plain) {
       it = 0;
-      dgf = perzyna_newton(P, vm, r.q_trial, r.q_y, (double)r.epd, dt, 0.01 * (r.q_trial - r.q_y) / P.f_mu_prefac, it, err);
+      dgf = solve(0.01 * ((double)r.q_trial - (double)r.q_y) / P.f_mu_prefac);
     }
     iters += it;
-    double hfin[3];
-    for (int j = 0; j < 3; ++j) hfin[j] = r.h[j] - (dgf / P.d_prefac) * r.hd[j];
+    float hfin[3];
+    for (int j = 0; j < 3; ++j) hfin[j] = (float)(r.h[j] - (dgf / P.d_prefac) * r.hd[j]);
     float Fout[9], tau[6];
     finish_F_tau(P, r.U, r.V, hfin, true, nullptr, Fout, tau);
     float* po = B.pout;
