@@ -1371,6 +1371,12 @@ pm_status pm_batch::upload_tables() {
   nl.n_g2p = g2p[n]; nl.n_def = def[n]; nl.n_sur = surv[n];
   nl.flat_threads = tune.flat_threads;
   nl.surrogate = sur;
+  // one plain-solver instantiation of the deformation update when every scene shares the model
+  nl.defgrad_model = h_sd[0].P.plastic_model;
+  for (int s = 0; s < n; ++s) {
+    const Params& q = h_sd[s].P;
+    if (q.plastic_model != nl.defgrad_model || q.return_map == 1 || q.log_cap > 0) nl.defgrad_model = -1;
+  }
   if (std::memcmp(&nl, &L, sizeof(BatchLaunch)) != 0) graph_dirty = true;
   L = nl;
   return PM_OK;

@@ -1470,10 +1470,12 @@ __device__ __forceinline__ void sur_features(const Params& P, const float h[3], 
 // The Newton path of the return map: either queue the particle for the surrogate, or solve
 // (VMVisc in FP32, DPVisc in FP64) and, when the sample log is on, record features and the
 // projected strains.
+// kExtras = false compiles out the surrogate queue and the sample log (plain-solver kernels).
+template <bool kExtras>
 __device__ bool newton_path(const Params& P, const Bufs& B, uint32_t i, bool vm, double dt, const float h[3],
                             const float hd[3], double q_trial, double q_yield, float epd, const float* U,
                             const float* V, double& dg, uint32_t& iters, uint32_t& err) {
-  if (P.return_map == 1 && P.q_cap > 0) {
+  if (kExtras && P.return_map == 1 && P.q_cap > 0) {
     const uint32_t slot = atomicAdd(&B.ctrl->q_n, 1u);
     if (slot < P.q_cap) {
       SurQ& r = B.q[slot];
@@ -1494,7 +1496,8 @@ __device__ bool newton_path(const Params& P, const Bufs& B, uint32_t i, bool vm,
   const double guess = 0.01 * (q_trial - q_yield) / P.f_mu_prefac;
   if (vm) dg = perzyna_newton_vm32(P, (float)q_trial, epd, (float)dt, (float)guess, iters, err);
   else dg = perzyna_newton(P, false, q_trial, q_yield, (double)epd, dt, guess, iters, err);
-  if (P.log_cap > 0 && (P.log_every <= 1 || ((i ^ (B.ctrl->step * 0x9E3779B9u)) * 0x85EBCA6Bu >> 8) % P.log_every == 0)) {
+  if (kExtras && P.log_cap > 0 &&
+      (P.log_every <= 1 || ((i ^ (B.ctrl->step * 0x9E3779B9u)) * 0x85EBCA6Bu >> 8) % P.log_every == 0)) {
     const uint32_t slot = atomicAdd(&B.ctrl->slog_n, 1u);
     if (slot < P.log_cap) {
       float* o = B.slog + (size_t)slot * 16;
@@ -1511,13 +1514,16 @@ __device__ bool newton_path(const Params& P, const Bufs& B, uint32_t i, bool vm,
 
 // plasticity.cpp:163-238 (VMVisc, FP32) and :240-340 (DPVisc, FP64: the cone and its apex).
 // sg: singular values of the trial elastic F (FP64 SVD); U, V its factors rounded to FP32.
+// kModel: the plastic model compiled in (PL_VMVISC, PL_DPVISC), or -1 to branch on P.plastic_model.
+template <int kModel, bool kExtras>
 __device__ void return_map(const Params& P, const Bufs& B, uint32_t i, double dt, const double sg[3], const float* U,
                            const float* V, float& epd, float& epv, float& epp, float& dgam, uint32_t& plastic,
                            uint32_t& iters, uint32_t& solves, uint32_t& err, ReturnMapOut& out) {
   out.changed = false;
   out.to_rotation = false;
   out.queued = false;
-  if (P.plastic_model == PL_VMVISC) {
+  const int model = kModel >= 0 ? kModel : P.plastic_model;
+  if (model == PL_VMVISC) {
     float h[3];
     for (int k = 0; k < 3; ++k) h[k] = logf(fmaxf(fabsf((float)sg[k]), 1e-4f));
     const float htr = h[0] + h[1] + h[2];
@@ -1547,7 +1553,10 @@ __device__ void return_map(const Params& P, const Bufs& B, uint32_t i, double dt
       } else {
         ++solves;
         double dgd = 0.0;
-        if (newton_path(P, B, i, true, dt, h, hd, q_trial, q_yield, epd, U, V, dgd, iters, err)) { out.queued = true; return; }
+        if (newton_path<kExtras>(P, B, i, true, dt, h, hd, q_trial, q_yield, epd, U, V, dgd, iters, err)) {
+          out.queued = true;
+          return;
+        }
         dg = (float)dgd;
       }
       for (int k = 0; k < 3; ++k) out.h[k] = h[k] - (dg / dpre) * hd[k];
@@ -1555,7 +1564,7 @@ __device__ void return_map(const Params& P, const Bufs& B, uint32_t i, double dt
       epd += dg / dpre;
       dgam = dg / dtf;
     }
-  } else if (P.plastic_model == PL_DPVISC) {
+  } else if (model == PL_DPVISC) {
     double h[3];
     for (int k = 0; k < 3; ++k) h[k] = log(fmax(fabs(sg[k]), 1e-4));
     const double htr = h[0] + h[1] + h[2];
@@ -1594,7 +1603,10 @@ __device__ void return_map(const Params& P, const Bufs& B, uint32_t i, double dt
         ++solves;
         const float hf[3] = {(float)h[0], (float)h[1], (float)h[2]};
         const float hdf[3] = {(float)hd[0], (float)hd[1], (float)hd[2]};
-        if (newton_path(P, B, i, false, dt, hf, hdf, q_trial, q_yield, epd, U, V, dg, iters, err)) { out.queued = true; return; }
+        if (newton_path<kExtras>(P, B, i, false, dt, hf, hdf, q_trial, q_yield, epd, U, V, dg, iters, err)) {
+          out.queued = true;
+          return;
+        }
       }
       for (int k = 0; k < 3; ++k) out.h[k] = (float)(h[k] - (dg / dpre) * hd[k]);
       out.changed = true;
@@ -1615,7 +1627,7 @@ __device__ __forceinline__ void finish_F_tau(const Params& P, const float* U, co
 #pragma unroll
       for (int q = 0; q < 3; ++q)
         Fout[3 * r + q] = U[3 * r] * e[0] * V[3 * q] + U[3 * r + 1] * e[1] * V[3 * q + 1] + U[3 * r + 2] * e[2] * V[3 * q + 2];
-  } else {
+  } else if (Ft) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) Fout[k] = Ft[k];
   }
@@ -1629,7 +1641,9 @@ __device__ __forceinline__ void finish_F_tau(const Params& P, const float* U, co
   tau[3] = T(0, 1); tau[4] = T(0, 2); tau[5] = T(1, 2);
 }
 
+template <int kModel, bool kExtras>
 __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
+  const int model = kModel >= 0 ? kModel : P.plastic_model;
   const Ctrl* c = B.ctrl;
   if (c->halt || c->idle) return;
   const int S = P.np_stride, np = P.np;
@@ -1755,10 +1769,10 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
         for (int k = 0; k < 3; ++k) s += (double)L[3 * r + k] * F[3 * k + q];
         Ft[3 * r + q] = F[3 * r + q] + dt * s;
       }
-    float epd = pi[F_EPD * S + o], epv = pi[F_EPV * S + o], epp = pi[F_EPP * S + o], dgam = 0.f;
-    float Ftf[9];  // F_trial as stored when the return map leaves it unchanged
+    // F_trial is the stored F unless the return map changes it (then it is overwritten below;
+    // both writes meet in L2), so it need not stay in registers across the SVD
 #pragma unroll
-    for (int k = 0; k < 9; ++k) Ftf[k] = (float)Ft[k];
+    for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = (float)Ft[k];
     double sg[3];
     float U[9], V[9];
     {
@@ -1767,11 +1781,13 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
 #pragma unroll
       for (int k = 0; k < 9; ++k) { U[k] = (float)Ud[k]; V[k] = (float)Vd[k]; }
     }
+    float epd = pi[F_EPD * S + o], epv = pi[F_EPV * S + o], epp = pi[F_EPP * S + o], dgam = 0.f;
     float hfin[3];
     bool changed = false, queued = false;
-    if (P.plastic_model != PL_NONE) {
+    if (model != PL_NONE) {
       ReturnMapOut rm;
-      return_map(P, B, (uint32_t)i, dt, sg, U, V, epd, epv, epp, dgam, plastic, niters, nsolves, err, rm);
+      return_map<kModel, kExtras>(P, B, (uint32_t)i, dt, sg, U, V, epd, epv, epp, dgam, plastic, niters, nsolves, err,
+                                  rm);
       changed = rm.changed;
       queued = rm.queued;
       if (rm.to_rotation) { hfin[0] = hfin[1] = hfin[2] = 0.f; }
@@ -1780,9 +1796,11 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     if (!changed) for (int k = 0; k < 3; ++k) hfin[k] = logf(fabsf((float)sg[k]));
     if (!queued) {  // queued particles get F, tau, eps_pl_dev and delta_gamma from the surrogate pass
       float Fout[9], tau[6];
-      finish_F_tau(P, U, V, hfin, changed, Ftf, Fout, tau);
+      finish_F_tau(P, U, V, hfin, changed, nullptr, Fout, tau);
+      if (changed) {
 #pragma unroll
-      for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = Fout[k];
+        for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = Fout[k];
+      }
 #pragma unroll
       for (int k = 0; k < 6; ++k) po[(F_TAU + k) * S + i] = tau[k];
       po[F_EPD * S + i] = epd;
@@ -1827,12 +1845,19 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     if (red_u[0][3]) atomicOr(&cw->error_flags, red_u[0][3]);
   }
 }
-__global__ void __launch_bounds__(kThreads, PM_DEFGRAD_MINB) k_defgrad(Params P, Bufs B) { d_defgrad(P, B, blockIdx.x, gridDim.x); }
-__global__ void __launch_bounds__(kThreads, PM_DEFGRAD_MINB) kb_defgrad(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+// Plain-solver instantiations per plastic model (kExtras = false) and the generic kernel (model
+// and extras chosen at run time) that the surrogate, the sample log and mixed batches use.
+template <int kModel, bool kExtras>
+__global__ void __launch_bounds__(kThreads, PM_DEFGRAD_MINB) k_defgrad(Params P, Bufs B) {
+  d_defgrad<kModel, kExtras>(P, B, blockIdx.x, gridDim.x);
+}
+template <int kModel, bool kExtras>
+__global__ void __launch_bounds__(kThreads, PM_DEFGRAD_MINB) kb_defgrad(const SceneDev* __restrict__ sd,
+                                                                        const int* __restrict__ off, int ns) {
   int s_, blk_, nblk_;
   batch_slot(off, ns, s_, blk_, nblk_);
   const SceneDev& d_ = sd[s_];
-  d_defgrad(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+  d_defgrad<kModel, kExtras>(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
 }
 
 
@@ -2004,7 +2029,7 @@ cudaError_t launch_init(int device) {
   if (e != cudaSuccess) return e;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_p2g, k_p2g, kThreads, p2g_smem_bytes());
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_g2p, k_g2p_musl, kThreads, g2p_smem_bytes());
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_def, k_defgrad, kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_def, k_defgrad<-1, true>, kThreads, 0);
   e = cudaFuncSetAttribute(kb_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem_bytes());
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(kb_g2p_musl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes());
@@ -2050,7 +2075,15 @@ void launch_step(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev
   k_p2g<<<sms * g_occ_p2g, kThreads, p2g_smem_bytes(), s>>>(P, B); mark();
   k_grid_update<<<flat_grid, 256, 0, s>>>(P, B); mark();
   k_g2p_musl<<<sms * g_occ_g2p, kThreads, g2p_smem_bytes(), s>>>(P, B); mark();
-  k_defgrad<<<sms * g_occ_def, kThreads, 0, s>>>(P, B); mark();
+  {
+    const int g = sms * g_occ_def;
+    const bool extras = P.return_map == 1 || P.log_cap > 0;
+    if (!extras && P.plastic_model == PL_VMVISC) k_defgrad<PL_VMVISC, false><<<g, kThreads, 0, s>>>(P, B);
+    else if (!extras && P.plastic_model == PL_DPVISC) k_defgrad<PL_DPVISC, false><<<g, kThreads, 0, s>>>(P, B);
+    else if (!extras && P.plastic_model == PL_NONE) k_defgrad<PL_NONE, false><<<g, kThreads, 0, s>>>(P, B);
+    else k_defgrad<-1, true><<<g, kThreads, 0, s>>>(P, B);
+    mark();
+  }
   if (P.return_map == 1) {
     mlp_infer(B.mlp, B.qx, B.qy, 0, &B.ctrl->q_n, (int)P.q_cap, s); mark();
     k_sur_finish<<<sms * 8, 128, 0, s>>>(P, B); mark();
@@ -2075,7 +2108,7 @@ void batched_occupancy(int& p2g, int& g2p, int& def) {
   p2g = g2p = def = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p2g, kb_p2g, kThreads, p2g_smem_bytes());
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g2p, kb_g2p_musl, kThreads, g2p_smem_bytes());
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&def, kb_defgrad, kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&def, kb_defgrad<-1, true>, kThreads, 0);
   p2g = p2g < 1 ? 1 : p2g;
   g2p = g2p < 1 ? 1 : g2p;
   def = def < 1 ? 1 : def;
@@ -2102,7 +2135,11 @@ void launch_step_batched(const BatchLaunch& L, cudaStream_t s, cudaEvent_t* ev) 
   kb_p2g<<<L.n_p2g, kThreads, p2g_smem_bytes(), s>>>(sd, L.off_p2g, ns); mark();
   kb_grid_update<<<L.n_node, ft, 0, s>>>(sd, L.off_node, ns); mark();
   kb_g2p_musl<<<L.n_g2p, kThreads, g2p_smem_bytes(), s>>>(sd, L.off_g2p, ns); mark();
-  kb_defgrad<<<L.n_def, kThreads, 0, s>>>(sd, L.off_def, ns); mark();
+  if (L.defgrad_model == PL_VMVISC) kb_defgrad<PL_VMVISC, false><<<L.n_def, kThreads, 0, s>>>(sd, L.off_def, ns);
+  else if (L.defgrad_model == PL_DPVISC) kb_defgrad<PL_DPVISC, false><<<L.n_def, kThreads, 0, s>>>(sd, L.off_def, ns);
+  else if (L.defgrad_model == PL_NONE) kb_defgrad<PL_NONE, false><<<L.n_def, kThreads, 0, s>>>(sd, L.off_def, ns);
+  else kb_defgrad<-1, true><<<L.n_def, kThreads, 0, s>>>(sd, L.off_def, ns);
+  mark();
   if (L.surrogate) {
     mlp_infer_batched(sd, L.off_sur, ns, L.n_sur, s); mark();
     kb_sur_finish<<<L.n_sur, 128, 0, s>>>(sd, L.off_sur, ns); mark();

@@ -38,6 +38,7 @@ struct BatchLaunch {
   int n_part = 0, n_node = 0, n_scan = 0, n_p2g = 0, n_g2p = 0, n_def = 0, n_sur = 0;
   int flat_threads = 256;         // block size of the flat kernels
   bool surrogate = false;         // some scene runs the learned return map
+  int defgrad_model = -1;         // plastic model shared by every scene on the plain solver, else -1
 };
 void launch_step_batched(const BatchLaunch& L, cudaStream_t s, cudaEvent_t* ev = nullptr);
 int batched_kernels_per_step(bool surrogate);
