@@ -563,6 +563,11 @@ constexpr int kThreads = 128;  // threads per CTA of the brick kernels
 #ifndef PM_G2P_MINB
 #define PM_G2P_MINB 6
 #endif
+// Unroll factor of the x-layer loop of the 27-node gathers (G2P, deformation update).
+#ifndef PM_GATHER_UNROLL_X
+#define PM_GATHER_UNROLL_X 3
+#endif
+constexpr int kGatherUnrollX = PM_GATHER_UNROLL_X;
 constexpr int kWarps = kThreads / 32;
 constexpr int kP2GCh = 15;
 
@@ -1089,14 +1094,16 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
         for (int k = 0; k < 9; ++k) { Bp[k] = 0.f; L[k] = 0.f; }
 #pragma unroll
         for (int k = 0; k < 7; ++k) gl[k] = 0.f;
-#pragma unroll
+#pragma unroll kGatherUnrollX
         for (int a = 0; a < 3; ++a) {
           const float dxa = (float)a * dx - aw[0].r;
+          const float Na = a == 0 ? aw[0].N[0] : (a == 1 ? aw[0].N[1] : aw[0].N[2]);
+          const float dNa = a == 0 ? aw[0].dN[0] : (a == 1 ? aw[0].dN[1] : aw[0].dN[2]);
 #pragma unroll
           for (int bb = 0; bb < 3; ++bb) {
             const float dyb = (float)bb * dx - aw[1].r;
-            const float nxy = aw[0].N[a] * aw[1].N[bb];
-            const float dnxy = aw[0].dN[a] * aw[1].N[bb], ndxy = aw[0].N[a] * aw[1].dN[bb];
+            const float nxy = Na * aw[1].N[bb];
+            const float dnxy = dNa * aw[1].N[bb], ndxy = Na * aw[1].dN[bb];
 #pragma unroll
             for (int cz = 0; cz < 3; ++cz) {
               const float dzc = (float)cz * dx - aw[2].r;
@@ -1229,62 +1236,8 @@ __global__ void __launch_bounds__(kThreads, PM_G2P_MINB) kb_g2p_musl(const Scene
 
 
 // ------------------------------------------------------------------------------------------
-// FP64 3x3 SVD (one-sided Jacobi, Hestenes) -- sigma >= 0, U, V orthogonal
+// FP64 3x3 SVD (warm-started one-sided Jacobi) -- sigma >= 0, U, V orthogonal
 // ------------------------------------------------------------------------------------------
-__device__ void svd3_d(const double A[9], double U[9], double s[3], double V[9]) {
-  double W[9];
-  for (int k = 0; k < 9; ++k) W[k] = A[k];
-  V[0] = 1; V[1] = 0; V[2] = 0; V[3] = 0; V[4] = 1; V[5] = 0; V[6] = 0; V[7] = 0; V[8] = 1;
-  const double eps = 2.220446049250313e-16;
-  for (int sweep = 0; sweep < 12; ++sweep) {
-    bool rotated = false;
-#pragma unroll
-    for (int pq = 0; pq < 3; ++pq) {
-      const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
-      double alpha = W[p] * W[p] + W[3 + p] * W[3 + p] + W[6 + p] * W[6 + p];
-      double beta = W[q] * W[q] + W[3 + q] * W[3 + q] + W[6 + q] * W[6 + q];
-      double gamma = W[p] * W[q] + W[3 + p] * W[3 + q] + W[6 + p] * W[6 + q];
-      if (gamma == 0.0 || fabs(gamma) <= eps * sqrt(alpha * beta)) continue;
-      rotated = true;
-      double zeta = (beta - alpha) / (2.0 * gamma);
-      double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-      double cs = rsqrt(1.0 + t * t);
-      double sn = cs * t;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        double wp = W[3 * k + p], wq = W[3 * k + q];
-        W[3 * k + p] = cs * wp - sn * wq;
-        W[3 * k + q] = sn * wp + cs * wq;
-        double vp = V[3 * k + p], vq = V[3 * k + q];
-        V[3 * k + p] = cs * vp - sn * vq;
-        V[3 * k + q] = sn * vp + cs * vq;
-      }
-    }
-    if (!rotated) break;
-  }
-  int valid = 0;
-  for (int j = 0; j < 3; ++j) {
-    s[j] = sqrt(W[j] * W[j] + W[3 + j] * W[3 + j] + W[6 + j] * W[6 + j]);
-  }
-  // left vectors; a column with zero norm is completed from the others
-  int zero_cols = 0;
-  int zc = -1;
-  for (int j = 0; j < 3; ++j) {
-    if (s[j] > 1e-300) {
-      double inv = 1.0 / s[j];
-      for (int k = 0; k < 3; ++k) U[3 * k + j] = W[3 * k + j] * inv;
-      ++valid;
-    } else { ++zero_cols; zc = j; }
-  }
-  if (zero_cols == 1) {
-    int a = (zc + 1) % 3, b = (zc + 2) % 3;
-    U[0 + zc] = U[3 + a] * U[6 + b] - U[6 + a] * U[3 + b];
-    U[3 + zc] = U[6 + a] * U[0 + b] - U[0 + a] * U[6 + b];
-    U[6 + zc] = U[0 + a] * U[3 + b] - U[3 + a] * U[0 + b];
-  } else if (zero_cols > 1) {
-    for (int k = 0; k < 9; ++k) U[k] = (k % 4 == 0) ? 1.0 : 0.0;
-  }
-}
 
 // FP32 cyclic Jacobi rotation of a symmetric 3x3 on pair (p, q); arp, arq are the entries of the
 // third row against p and q; V accumulates the rotations.
@@ -1311,9 +1264,13 @@ __device__ __forceinline__ void jrot_f32(float& app, float& aqq, float& apq, flo
 
 // SVD of a 3x3 with an FP32 warm start: cyclic Jacobi in FP32 on the trace-shifted A^T A gives
 // approximate right singular vectors; they are re-orthonormalised in FP64 and one-sided Jacobi
-// sweeps in FP64 run on W = A V until no column pair needs a rotation, so the result has FP64
-// accuracy (sigma >= 0, U and V orthogonal) with fewer FP64 rotations than a cold start.
-__device__ void svd3_warm(const double A[9], double U[9], double s[3], double V[9]) {
+// (Hestenes) sweeps in FP64 run on W = A V until no column pair needs a rotation, so the singular
+// values have FP64 accuracy and U, V are orthogonal to FP64 rounding before they are rounded to
+// the FP32 factors the rest of the step uses.  Near convergence a rotation angle only has to be
+// accurate to first order: (cos, sin) are computed in FP32 from the FP64 column products and
+// renormalised in FP64 by one Newton step on cos^2 + sin^2 = 1 (error O(1e-14)), which replaces
+// the FP64 divide, square root and reciprocal square root of each rotation.
+__device__ void svd3_warm(const double A[9], float Uf[9], double s[3], float Vf_out[9]) {
   double S[6];
   S[0] = A[0] * A[0] + A[3] * A[3] + A[6] * A[6];
   S[1] = A[1] * A[1] + A[4] * A[4] + A[7] * A[7];
@@ -1334,21 +1291,24 @@ __device__ void svd3_warm(const double A[9], double U[9], double s[3], double V[
     if (off <= 1e-7f * (fabsf(a00) + fabsf(a11) + fabsf(a22)) + 1e-30f) break;
   }
   // FP64 Gram-Schmidt of the FP32 rotation -> orthonormal V0 (det +1)
-  double v0[3] = {Vf[0], Vf[3], Vf[6]}, v1[3] = {Vf[1], Vf[4], Vf[7]};
-  const double n0 = rsqrt(v0[0] * v0[0] + v0[1] * v0[1] + v0[2] * v0[2]);
-  for (int k = 0; k < 3; ++k) v0[k] *= n0;
-  const double d01 = v0[0] * v1[0] + v0[1] * v1[1] + v0[2] * v1[2];
-  for (int k = 0; k < 3; ++k) v1[k] -= d01 * v0[k];
-  const double n1 = rsqrt(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]);
-  for (int k = 0; k < 3; ++k) v1[k] *= n1;
-  const double v2[3] = {v0[1] * v1[2] - v0[2] * v1[1], v0[2] * v1[0] - v0[0] * v1[2], v0[0] * v1[1] - v0[1] * v1[0]};
-  for (int k = 0; k < 3; ++k) { V[3 * k] = v0[k]; V[3 * k + 1] = v1[k]; V[3 * k + 2] = v2[k]; }
+  double V[9];
+  {
+    double v0[3] = {Vf[0], Vf[3], Vf[6]}, v1[3] = {Vf[1], Vf[4], Vf[7]};
+    const double n0 = rsqrt(v0[0] * v0[0] + v0[1] * v0[1] + v0[2] * v0[2]);
+    for (int k = 0; k < 3; ++k) v0[k] *= n0;
+    const double d01 = v0[0] * v1[0] + v0[1] * v1[1] + v0[2] * v1[2];
+    for (int k = 0; k < 3; ++k) v1[k] -= d01 * v0[k];
+    const double n1 = rsqrt(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]);
+    for (int k = 0; k < 3; ++k) v1[k] *= n1;
+    const double v2[3] = {v0[1] * v1[2] - v0[2] * v1[1], v0[2] * v1[0] - v0[0] * v1[2], v0[0] * v1[1] - v0[1] * v1[0]};
+    for (int k = 0; k < 3; ++k) { V[3 * k] = v0[k]; V[3 * k + 1] = v1[k]; V[3 * k + 2] = v2[k]; }
+  }
   double W[9];
 #pragma unroll
   for (int r = 0; r < 3; ++r)
 #pragma unroll
     for (int q = 0; q < 3; ++q) W[3 * r + q] = A[3 * r] * V[q] + A[3 * r + 1] * V[3 + q] + A[3 * r + 2] * V[6 + q];
-  const double eps = 2.220446049250313e-16;
+  const double eps2 = 2.220446049250313e-16 * 2.220446049250313e-16;
 #pragma unroll 1
   for (int sweep = 0; sweep < 8; ++sweep) {
     bool rotated = false;
@@ -1358,12 +1318,15 @@ __device__ void svd3_warm(const double A[9], double U[9], double s[3], double V[
       const double alpha = W[p] * W[p] + W[3 + p] * W[3 + p] + W[6 + p] * W[6 + p];
       const double beta = W[q] * W[q] + W[3 + q] * W[3 + q] + W[6 + q] * W[6 + q];
       const double gamma = W[p] * W[q] + W[3 + p] * W[3 + q] + W[6 + p] * W[6 + q];
-      if (gamma == 0.0 || fabs(gamma) <= eps * sqrt(alpha * beta)) continue;
+      if (gamma == 0.0 || gamma * gamma <= eps2 * alpha * beta) continue;
       rotated = true;
-      const double zeta = (beta - alpha) / (2.0 * gamma);
-      const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-      const double cs = rsqrt(1.0 + t * t);
-      const double sn = cs * t;
+      const float zeta = (float)(beta - alpha) / (2.f * (float)gamma);
+      const float t = copysignf(1.f, zeta) / (fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.f)));
+      const float csf = rsqrtf(fmaf(t, t, 1.f));
+      double cs = csf, sn = (double)(csf * t);
+      const double f = 1.5 - 0.5 * (cs * cs + sn * sn);
+      cs *= f;
+      sn *= f;
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         const double wp = W[3 * k + p], wq = W[3 * k + q];
@@ -1376,21 +1339,32 @@ __device__ void svd3_warm(const double A[9], double U[9], double s[3], double V[
     }
     if (!rotated) break;
   }
-  int zero_cols = 0, zc = -1;
+  // singular values in FP64; U = W diag(1/s) and V rounded to FP32 (fixed indices throughout, so
+  // the factors stay in registers)
+  bool ok[3];
+#pragma unroll
   for (int j = 0; j < 3; ++j) {
     s[j] = sqrt(W[j] * W[j] + W[3 + j] * W[3 + j] + W[6 + j] * W[6 + j]);
-    if (s[j] > 1e-300) {
-      const double inv = 1.0 / s[j];
-      for (int k = 0; k < 3; ++k) U[3 * k + j] = W[3 * k + j] * inv;
-    } else { ++zero_cols; zc = j; }
+    ok[j] = s[j] > 1e-300;
+    const float inv = ok[j] ? (float)(1.0 / s[j]) : 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Uf[3 * k + j] = (float)W[3 * k + j] * inv;
   }
-  if (zero_cols == 1) {
-    const int a = (zc + 1) % 3, b = (zc + 2) % 3;
-    U[0 + zc] = U[3 + a] * U[6 + b] - U[6 + a] * U[3 + b];
-    U[3 + zc] = U[6 + a] * U[0 + b] - U[0 + a] * U[6 + b];
-    U[6 + zc] = U[0 + a] * U[3 + b] - U[3 + a] * U[0 + b];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) Vf_out[k] = (float)V[k];
+  const int zero_cols = (!ok[0]) + (!ok[1]) + (!ok[2]);
+  if (zero_cols == 1) {  // complete U with the cross product of its other two columns
+    auto cross_col = [&](int z, int a, int b) {
+      Uf[0 + z] = Uf[3 + a] * Uf[6 + b] - Uf[6 + a] * Uf[3 + b];
+      Uf[3 + z] = Uf[6 + a] * Uf[0 + b] - Uf[0 + a] * Uf[6 + b];
+      Uf[6 + z] = Uf[0 + a] * Uf[3 + b] - Uf[3 + a] * Uf[0 + b];
+    };
+    if (!ok[0]) cross_col(0, 1, 2);
+    else if (!ok[1]) cross_col(1, 2, 0);
+    else cross_col(2, 0, 1);
   } else if (zero_cols > 1) {
-    for (int k = 0; k < 9; ++k) U[k] = (k % 4 == 0) ? 1.0 : 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Uf[k] = (k % 4 == 0) ? 1.f : 0.f;
   }
 }
 
@@ -1676,28 +1650,35 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
       xp[d] = pi[(F_X + d) * S + o];
       aw[d] = axis_weights(xp[d], P.anchor[d], dx, P.inv_dx);
     }
-    // node indices of the stencil per axis
-    int bidx[3][3], lidx[3][3];
+    // node index of the stencil = off[0][a] + off[1][b] + off[2][c]: each axis contributes its
+    // brick stride and its position inside the brick
+    int off[3][3];
+    {
+      const int bs[3] = {c->nb[1] * c->nb[2] * kBrickNodes, c->nb[2] * kBrickNodes, kBrickNodes};
 #pragma unroll
-    for (int d = 0; d < 3; ++d)
+      for (int d = 0; d < 3; ++d)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        int n = min(max(aw[d].base + k - c->g0[d], 0), c->dims[d] - 1);  // inside the box by construction
-        bidx[d][k] = n >> 2;
-        lidx[d][k] = n & 3;
-      }
+        for (int k = 0; k < 3; ++k) {
+          const int n = min(max(aw[d].base + k - c->g0[d], 0), c->dims[d] - 1);  // inside the box by construction
+          off[d][k] = (n >> 2) * bs[d] + (n & 3) * (d == 0 ? 16 : (d == 1 ? 4 : 1));
+        }
+    }
     // velocity gradient from the MUSL grid (deformation_update.cpp:26-39)
     float L[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) L[k] = 0.f;
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
+    // the x-layer loop stays rolled (kGatherUnrollX) to keep the kernel's code small; its per-layer
+    // values are picked with selects, not indexed, so they stay in registers
+#pragma unroll kGatherUnrollX
+    for (int a = 0; a < 3; ++a) {
+      const float Na = a == 0 ? aw[0].N[0] : (a == 1 ? aw[0].N[1] : aw[0].N[2]);
+      const float dNa = a == 0 ? aw[0].dN[0] : (a == 1 ? aw[0].dN[1] : aw[0].dN[2]);
+      const int oa = a == 0 ? off[0][0] : (a == 1 ? off[0][1] : off[0][2]);
 #pragma unroll
       for (int bb = 0; bb < 3; ++bb)
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
-          const int node = ((bidx[0][a] * c->nb[1] + bidx[1][bb]) * c->nb[2] + bidx[2][cc]) * kBrickNodes +
-                           lidx[0][a] * 16 + lidx[1][bb] * 4 + lidx[2][cc];
+          const int node = oa + off[1][bb] + off[2][cc];
           float gv[3];
           if (P.use_musl) {
             const float4 m = B.gmusl[node];
@@ -1707,13 +1688,14 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
             const float4 m = B.grid[(size_t)node * 4];
             gv[0] = m.x; gv[1] = m.y; gv[2] = m.z;
           }
-          const float g[3] = {aw[0].dN[a] * aw[1].N[bb] * aw[2].N[cc], aw[0].N[a] * aw[1].dN[bb] * aw[2].N[cc],
-                              aw[0].N[a] * aw[1].N[bb] * aw[2].dN[cc]};
+          const float g[3] = {dNa * aw[1].N[bb] * aw[2].N[cc], Na * aw[1].dN[bb] * aw[2].N[cc],
+                              Na * aw[1].N[bb] * aw[2].dN[cc]};
 #pragma unroll
           for (int r = 0; r < 3; ++r)
 #pragma unroll
             for (int q = 0; q < 3; ++q) L[3 * r + q] += gv[r] * g[q];
         }
+    }
     // position update (position_update.cpp:6-91); done before the SVD so that its values are not
     // live across it
     float pic[3], v[3];
@@ -1775,12 +1757,7 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = (float)Ft[k];
     double sg[3];
     float U[9], V[9];
-    {
-      double Ud[9], Vd[9];
-      svd3_warm(Ft, Ud, sg, Vd);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) { U[k] = (float)Ud[k]; V[k] = (float)Vd[k]; }
-    }
+    svd3_warm(Ft, U, sg, V);
     float epd = pi[F_EPD * S + o], epv = pi[F_EPV * S + o], epp = pi[F_EPP * S + o], dgam = 0.f;
     float hfin[3];
     bool changed = false, queued = false;
