@@ -1372,6 +1372,8 @@ pm_status pm_batch::upload_tables() {
   nl.flat_threads = tune.flat_threads;
   nl.surrogate = sur;
   // one plain-solver instantiation of the deformation update when every scene shares the model
+  nl.g2p_flip = false;
+  for (int s = 0; s < n; ++s) nl.g2p_flip = nl.g2p_flip || h_sd[s].P.flip_ratio >= -1.f;
   nl.defgrad_model = h_sd[0].P.plastic_model;
   for (int s = 0; s < n; ++s) {
     const Params& q = h_sd[s].P;

@@ -660,7 +660,10 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
     if (ps == pe) continue;
     int bx, by, bz;
     brick_coords(b, c, bx, by, bz);
-    for (int i = threadIdx.x; i < kP2GCh * kTileStride; i += kThreads) tile[i] = 0.f;
+    {
+      float4* t4 = reinterpret_cast<float4*>(tile);  // kP2GCh * kTileStride is a multiple of 4
+      for (int i = threadIdx.x; i < kP2GCh * kTileStride / 4; i += kThreads) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     __syncthreads();
     for (uint32_t c0 = ps + 32u * warp; c0 < pe; c0 += 32u * kWarps) {
       const int n = (int)min(32u, pe - c0);
@@ -1031,6 +1034,9 @@ __device__ __forceinline__ float smooth_step(float e0, float e1, float x) {  // 
 // gathers G2P for particle i, writes its new state in sorted order and stages its MUSL data; the
 // warp then scatters the staged particles run by run of equal cells, lane l < 27 owning stencil
 // node l, into the brick's shared MUSL tile, flushed once per brick.
+// kFlip: FLIP blending in use (flip_ratio >= -1); false compiles the pure-APIC kernel, which
+// neither reads the old particle velocity nor gathers the grid's velocity change.
+template <bool kFlip>
 __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
   if (c->halt || c->idle) return;
@@ -1046,7 +1052,7 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
   const StencilPoly px(la, P.inv_dx), py(lb, P.inv_dx), pz(lc, P.inv_dx);
   const float D = P.apicD, dx = P.dx;
   const float fr = P.flip_ratio;
-  const bool apic = fr < 0.f, use_flip = fr >= -1.f, musl = P.use_musl != 0;
+  const bool apic = fr < 0.f, use_flip = kFlip, musl = P.use_musl != 0;
   const float dtf = (float)c->dt;
   // pigment mixing factor pieces (g2p.cpp:105-119)
   float time_factor = 1.f;
@@ -1069,7 +1075,10 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
       const int node = tile_to_node(i >> 2, bx, by, bz, c);
       tile[i] = node >= 0 ? B.grid[(size_t)node * 4 + (i & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    for (int i = threadIdx.x; i < 4 * kTileStride; i += kThreads) mtile[i] = 0.f;
+    {
+      float4* m4 = reinterpret_cast<float4*>(mtile);
+      for (int i = threadIdx.x; i < kTileStride; i += kThreads) m4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     __syncthreads();
     for (uint32_t c0 = ps + 32u * warp; c0 < pe; c0 += 32u * kWarps) {
       const int n = (int)min(32u, pe - c0);
@@ -1077,16 +1086,10 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
       if (lane < n) {
         const uint32_t i = c0 + lane;
         const uint32_t o = B.sorted[i];
-        float xp[3], vold[3], lat[7];
+        float lat[7];
         AxisW aw[3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          xp[d] = B.pin[(F_X + d) * S + o];
-          vold[d] = B.pin[(F_V + d) * S + o];
-          aw[d] = axis_weights(xp[d], P.anchor[d], dx, P.inv_dx);
-        }
-#pragma unroll
-        for (int k = 0; k < 7; ++k) lat[k] = B.pin[(F_LAT + k) * S + o];
+        for (int d = 0; d < 3; ++d) aw[d] = axis_weights(B.pin[(F_X + d) * S + o], P.anchor[d], dx, P.inv_dx);
         cl = local_cell(aw, c, bx, by, bz);
         const int lx = cl >> 4, ly = (cl >> 2) & 3, lz = cl & 3;
         float vp[3] = {0.f, 0.f, 0.f}, fp[3] = {0.f, 0.f, 0.f}, Bp[9], L[9], gl[7], gs = 0.f;
@@ -1132,6 +1135,14 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
           }
         }
         if (!apic) for (int k = 0; k < 9; ++k) Bp[k] = 0.f;
+        // particle state read after the gather (not live across it)
+#pragma unroll
+        for (int k = 0; k < 7; ++k) lat[k] = B.pin[(F_LAT + k) * S + o];
+        float vold[3] = {0.f, 0.f, 0.f};
+        if (kFlip || !musl) {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) vold[d] = B.pin[(F_V + d) * S + o];
+        }
         // diffusion factor |0.5 (L + L^T)|_F (g2p.cpp:98-101)
         float s2 = 0.f;
 #pragma unroll
@@ -1226,12 +1237,17 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
     __syncthreads();
   }
 }
-__global__ void __launch_bounds__(kThreads, PM_G2P_MINB) k_g2p_musl(Params P, Bufs B) { d_g2p_musl(P, B, blockIdx.x, gridDim.x); }
-__global__ void __launch_bounds__(kThreads, PM_G2P_MINB) kb_g2p_musl(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
+template <bool kFlip>
+__global__ void __launch_bounds__(kThreads, PM_G2P_MINB) k_g2p_musl(Params P, Bufs B) {
+  d_g2p_musl<kFlip>(P, B, blockIdx.x, gridDim.x);
+}
+template <bool kFlip>
+__global__ void __launch_bounds__(kThreads, PM_G2P_MINB) kb_g2p_musl(const SceneDev* __restrict__ sd,
+                                                                     const int* __restrict__ off, int ns) {
   int s_, blk_, nblk_;
   batch_slot(off, ns, s_, blk_, nblk_);
   const SceneDev& d_ = sd[s_];
-  d_g2p_musl(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+  d_g2p_musl<kFlip>(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
 }
 
 
@@ -2002,15 +2018,17 @@ cudaError_t launch_init(int device) {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem_bytes());
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_g2p_musl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes());
-  if (e != cudaSuccess) return e;
+  for (const void* f : {(const void*)k_g2p_musl<true>, (const void*)k_g2p_musl<false>, (const void*)kb_g2p_musl<true>,
+                        (const void*)kb_g2p_musl<false>}) {
+    e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes());
+    if (e != cudaSuccess) return e;
+  }
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_p2g, k_p2g, kThreads, p2g_smem_bytes());
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_g2p, k_g2p_musl, kThreads, g2p_smem_bytes());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_g2p, k_g2p_musl<true>, kThreads, g2p_smem_bytes());
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ_def, k_defgrad<-1, true>, kThreads, 0);
   e = cudaFuncSetAttribute(kb_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem_bytes());
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(kb_g2p_musl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes());
-  if (e != cudaSuccess) return e;
+
   e = mlp_init();
   if (e != cudaSuccess) return e;
   if (g_occ_p2g < 1) g_occ_p2g = 1;
@@ -2051,7 +2069,9 @@ void launch_step(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev
   k_clear_bricks<<<flat_grid, 256, 0, s>>>(P, B); mark();
   k_p2g<<<sms * g_occ_p2g, kThreads, p2g_smem_bytes(), s>>>(P, B); mark();
   k_grid_update<<<flat_grid, 256, 0, s>>>(P, B); mark();
-  k_g2p_musl<<<sms * g_occ_g2p, kThreads, g2p_smem_bytes(), s>>>(P, B); mark();
+  if (P.flip_ratio >= -1.f) k_g2p_musl<true><<<sms * g_occ_g2p, kThreads, g2p_smem_bytes(), s>>>(P, B);
+  else k_g2p_musl<false><<<sms * g_occ_g2p, kThreads, g2p_smem_bytes(), s>>>(P, B);
+  mark();
   {
     const int g = sms * g_occ_def;
     const bool extras = P.return_map == 1 || P.log_cap > 0;
@@ -2084,7 +2104,7 @@ const char* batched_kernel_name(int i, bool surrogate) {
 void batched_occupancy(int& p2g, int& g2p, int& def) {
   p2g = g2p = def = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p2g, kb_p2g, kThreads, p2g_smem_bytes());
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g2p, kb_g2p_musl, kThreads, g2p_smem_bytes());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g2p, kb_g2p_musl<true>, kThreads, g2p_smem_bytes());
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&def, kb_defgrad<-1, true>, kThreads, 0);
   p2g = p2g < 1 ? 1 : p2g;
   g2p = g2p < 1 ? 1 : g2p;
@@ -2111,7 +2131,9 @@ void launch_step_batched(const BatchLaunch& L, cudaStream_t s, cudaEvent_t* ev) 
   kb_clear_bricks<<<L.n_node, ft, 0, s>>>(sd, L.off_node, ns); mark();
   kb_p2g<<<L.n_p2g, kThreads, p2g_smem_bytes(), s>>>(sd, L.off_p2g, ns); mark();
   kb_grid_update<<<L.n_node, ft, 0, s>>>(sd, L.off_node, ns); mark();
-  kb_g2p_musl<<<L.n_g2p, kThreads, g2p_smem_bytes(), s>>>(sd, L.off_g2p, ns); mark();
+  if (L.g2p_flip) kb_g2p_musl<true><<<L.n_g2p, kThreads, g2p_smem_bytes(), s>>>(sd, L.off_g2p, ns);
+  else kb_g2p_musl<false><<<L.n_g2p, kThreads, g2p_smem_bytes(), s>>>(sd, L.off_g2p, ns);
+  mark();
   if (L.defgrad_model == PL_VMVISC) kb_defgrad<PL_VMVISC, false><<<L.n_def, kThreads, 0, s>>>(sd, L.off_def, ns);
   else if (L.defgrad_model == PL_DPVISC) kb_defgrad<PL_DPVISC, false><<<L.n_def, kThreads, 0, s>>>(sd, L.off_def, ns);
   else if (L.defgrad_model == PL_NONE) kb_defgrad<PL_NONE, false><<<L.n_def, kThreads, 0, s>>>(sd, L.off_def, ns);

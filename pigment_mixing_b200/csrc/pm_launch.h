@@ -39,6 +39,7 @@ struct BatchLaunch {
   int flat_threads = 256;         // block size of the flat kernels
   bool surrogate = false;         // some scene runs the learned return map
   int defgrad_model = -1;         // plastic model shared by every scene on the plain solver, else -1
+  bool g2p_flip = true;           // some scene blends FLIP (flip_ratio >= -1)
 };
 void launch_step_batched(const BatchLaunch& L, cudaStream_t s, cudaEvent_t* ev = nullptr);
 int batched_kernels_per_step(bool surrogate);
