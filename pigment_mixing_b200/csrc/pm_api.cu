@@ -926,6 +926,20 @@ pm_status pm_prepare(pm_sim* sim) {
       nb *= n;
     }
     long long want = nb * 2 + 64;
+    // With particle boundaries the grid box can never outgrow the boundary box: allocate that box
+    // once (about 88 B per node) when it takes at most 1/8 of the free device memory, so long runs
+    // never stop to regrow.
+    if (h.use_particle_boundaries) {
+      long long nbb = 1;
+      for (int d = 0; d < 3; ++d) {
+        const long long n = (long long)std::ceil((h.pbmax[d] - h.pbmin[d]) / h.dx) + 8;
+        nbb *= (n + 3) / 4 + 1;
+      }
+      size_t free_b = 0, total_b = 0;
+      if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && nbb > want &&
+          (double)nbb * kBrickNodes * 88.0 <= 0.125 * (double)free_b)
+        want = nbb;
+    }
     if (want * kBrickNodes > 0x7ffffff0LL) want = 0x7ffffff0LL / kBrickNodes;
     if (sim->brick_cap < want) {
       if ((s = sim->alloc_grid((int)want)) != PM_OK) return s;

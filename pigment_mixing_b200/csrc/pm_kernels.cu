@@ -558,7 +558,7 @@ constexpr int kThreads = 128;  // threads per CTA of the brick kernels
 // is sized for (launch bounds): more CTAs hide more latency, fewer leave registers for the
 // FP64 SVD.
 #ifndef PM_DEFGRAD_MINB
-#define PM_DEFGRAD_MINB 5
+#define PM_DEFGRAD_MINB 8
 #endif
 #ifndef PM_G2P_MINB
 #define PM_G2P_MINB 6
@@ -1645,20 +1645,15 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
   int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
   const int stride = nblk_ * blockDim.x;
   const float fr = P.flip_ratio;
-  for (int i = blk_ * blockDim.x + threadIdx.x; i < np; i += stride) {
+  // grid velocities of the brick's 6x6x6 stencil tile: the MUSL velocity (normalised once per
+  // node here) or, in USL mode, the updated grid velocity
+  __shared__ float4 vt[kTileNodes];
+  int bx = 0, by = 0, bz = 0;
+  float* po = B.pout;
+  const float* pi = B.pin;
+  auto particle = [&](const int i) {
     const uint32_t o = B.sorted[i];
     const uint32_t meta = B.meta_in[o];
-    float* po = B.pout;
-    const float* pi = B.pin;
-    if (meta & kInactiveBit) {  // carried through unchanged (G2P zeroes B, deformation update zeroes delta_gamma)
-      for (int f = 0; f < F_COUNT; ++f) {
-        float v = pi[f * S + o];
-        if ((f >= F_B && f < F_B + 9) || f == F_DG) v = 0.f;
-        po[f * S + i] = v;
-      }
-      B.meta_out[i] = meta;
-      continue;
-    }
     float xp[3];
     AxisW aw[3];
 #pragma unroll
@@ -1666,44 +1661,24 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
       xp[d] = pi[(F_X + d) * S + o];
       aw[d] = axis_weights(xp[d], P.anchor[d], dx, P.inv_dx);
     }
-    // node index of the stencil = off[0][a] + off[1][b] + off[2][c]: each axis contributes its
-    // brick stride and its position inside the brick
-    int off[3][3];
-    {
-      const int bs[3] = {c->nb[1] * c->nb[2] * kBrickNodes, c->nb[2] * kBrickNodes, kBrickNodes};
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const int n = min(max(aw[d].base + k - c->g0[d], 0), c->dims[d] - 1);  // inside the box by construction
-          off[d][k] = (n >> 2) * bs[d] + (n & 3) * (d == 0 ? 16 : (d == 1 ? 4 : 1));
-        }
-    }
+    const int cl = local_cell(aw, c, bx, by, bz);
+    const int t0 = ((cl >> 4) * kTile + ((cl >> 2) & 3)) * kTile + (cl & 3);
     // velocity gradient from the MUSL grid (deformation_update.cpp:26-39)
     float L[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) L[k] = 0.f;
-    // the x-layer loop stays rolled (kGatherUnrollX) to keep the kernel's code small; its per-layer
-    // values are picked with selects, not indexed, so they stay in registers
+    // the x-layer loop may stay rolled (kGatherUnrollX) to keep the kernel's code small; its
+    // per-layer values are picked with selects, not indexed, so they stay in registers
 #pragma unroll kGatherUnrollX
     for (int a = 0; a < 3; ++a) {
       const float Na = a == 0 ? aw[0].N[0] : (a == 1 ? aw[0].N[1] : aw[0].N[2]);
       const float dNa = a == 0 ? aw[0].dN[0] : (a == 1 ? aw[0].dN[1] : aw[0].dN[2]);
-      const int oa = a == 0 ? off[0][0] : (a == 1 ? off[0][1] : off[0][2]);
 #pragma unroll
       for (int bb = 0; bb < 3; ++bb)
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
-          const int node = oa + off[1][bb] + off[2][cc];
-          float gv[3];
-          if (P.use_musl) {
-            const float4 m = B.gmusl[node];
-            const float inv = m.w > 0.f ? 1.f / m.w : 0.f;
-            gv[0] = m.x * inv; gv[1] = m.y * inv; gv[2] = m.z * inv;
-          } else {
-            const float4 m = B.grid[(size_t)node * 4];
-            gv[0] = m.x; gv[1] = m.y; gv[2] = m.z;
-          }
+          const float4 m = vt[t0 + (a * kTile + bb) * kTile + cc];
+          const float gv[3] = {m.x, m.y, m.z};
           const float g[3] = {dNa * aw[1].N[bb] * aw[2].N[cc], Na * aw[1].dN[bb] * aw[2].N[cc],
                               Na * aw[1].N[bb] * aw[2].dN[cc]};
 #pragma unroll
@@ -1801,6 +1776,41 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     }
     po[F_EPV * S + i] = epv;
     po[F_EPP * S + i] = epp;
+  };
+  const int nbr = c->n_bricks;
+  for (int b = blk_; b < nbr; b += nblk_) {
+    const uint32_t ps = B.cell[(size_t)b * kBrickNodes], pe = B.cell[(size_t)(b + 1) * kBrickNodes];
+    if (ps == pe) continue;
+    brick_coords(b, c, bx, by, bz);
+    __syncthreads();  // the previous brick's readers are done with the tile
+    for (int tn = threadIdx.x; tn < kTileNodes; tn += blockDim.x) {
+      const int node = tile_to_node(tn, bx, by, bz, c);
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (node >= 0) {
+        if (P.use_musl) {
+          const float4 m = B.gmusl[node];
+          const float inv = m.w > 0.f ? 1.f / m.w : 0.f;
+          v = make_float4(m.x * inv, m.y * inv, m.z * inv, 0.f);
+        } else {
+          const float4 m = B.grid[(size_t)node * 4];
+          v = make_float4(m.x, m.y, m.z, 0.f);
+        }
+      }
+      vt[tn] = v;
+    }
+    __syncthreads();
+    for (int i = (int)ps + threadIdx.x; i < (int)pe; i += blockDim.x) particle(i);
+  }
+  // inactive particles sit behind every brick in the sorted order: carried through unchanged
+  // (G2P zeroes B, the deformation update zeroes delta_gamma)
+  for (int i = (int)B.cell[c->n_nodes] + blk_ * blockDim.x + threadIdx.x; i < np; i += stride) {
+    const uint32_t o = B.sorted[i];
+    for (int f = 0; f < F_COUNT; ++f) {
+      float v = pi[f * S + o];
+      if ((f >= F_B && f < F_B + 9) || f == F_DG) v = 0.f;
+      po[f * S + i] = v;
+    }
+    B.meta_out[i] = B.meta_in[o];
   }
   // block reduction, then one set of atomics per block
   __shared__ int red_i[kWarps][8];

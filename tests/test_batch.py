@@ -96,6 +96,7 @@ def test_batch_regrows_one_scene_and_keeps_the_others_in_step():
     sc = scenes.two_block_scene(1.0 / 32, (4, 4, 4), seed=5, steps=10, knife=False, material="vmvisc")
     sc["params"].update(plastic_model=0, E=1.0, rho=1000.0, particle_mass=1000.0 * (1.0 / 32) ** 3 / 8.0)
     sc["vectors"]["gravity"] = [0.0, 0.0, 0.0]
+    sc["params"]["use_particle_boundaries"] = 0  # unbounded: the grid is sized from the blocks and must grow
     c = sc["x"].mean(0)
     c[1] = 0.0
     v = (3.0 * (sc["x"] - c)).astype(np.float32)
