@@ -52,6 +52,8 @@ def _workload(name: str):
         return scenes.config3(seed=0)
     if name == "32k":
         return scenes.config1(seed=0)
+    if name == "32m":
+        return scenes.config5(seed=0)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -263,14 +265,20 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+_BLOCKS = {"2m": "two 64x64x32-cell blocks", "32k": "two 16x16x8-cell blocks",
+           "8m": "four 64^3-cell blocks of four pigments", "32m": "six 87^3-cell blocks (3 x 2) of six pigments"}
+_PATH = {"2m": "a 3-segment path", "32k": "a 3-segment path", "8m": "a 3-segment path",
+         "32m": "four back-and-forth strokes"}
+
+
 def _config(scene, args):
     n = len(scene["x"])
-    return {"workload": f"{scene['name']}: {n} particles, dx={scene['params']['dx']:.6g}, two cuboid paint blocks, "
-                        "VMVisc (Herschel-Bulkley) paint, box knife 0.4x0.2x0.01 on a 3-segment path at 0.5 u/s, "
-                        "MUSL, APIC",
+    return {"workload": f"{scene['name']}: {n} particles, dx={scene['params']['dx']:.6g}, "
+                        f"{_BLOCKS[args.workload]}, VMVisc (Herschel-Bulkley) paint, box knife 0.4x0.2x0.01 on "
+                        f"{_PATH[args.workload]} at 0.5 u/s, MUSL, APIC",
             "particles": n, "return_map": args.return_map,
-            "precision": "FP32 transfers and grid, FP64 SVD and return map",
-            "l2": "inputs larger than L2 (particle state 0.35 GB per buffer at 2M particles)",
+            "precision": "FP32 transfers, grid and VMVisc return map; FP64 SVD of the elastic F",
+            "l2": f"inputs larger than L2 (particle state {n * 168 / 1e9:.2f} GB per buffer, L2 126 MB)",
             "parallelism": f"replicas x{args.gpus}"}
 
 
@@ -559,7 +567,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="2m", choices=["2m", "8m", "32k"])
+    ap.add_argument("--workload", default="2m", choices=["2m", "8m", "32k", "32m"])
     ap.add_argument("--return-map", default="plain", choices=["plain"],
                     help="return map of the headline value (the surrogate form is reported beside it)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

@@ -1,14 +1,14 @@
 """Profiling driver: per-kernel CUDA-event times of the step on a named workload, followed by a
 few plain (non-graph) steps that an external profiler can capture.
 
-    python -m pigment_mixing_b200.profile_step [--workload 2m|8m|32k] [--warm 10] [--profile 3] [--plain 3]
+    python -m pigment_mixing_b200.profile_step [--workload 2m|8m|32k|32m] [--warm 10] [--profile 3] [--plain 3]
 """
 import argparse
 import json
 
 from . import Simulation, scenes
 
-WORKLOADS = {"2m": scenes.config2, "8m": scenes.config3, "32k": scenes.config1}
+WORKLOADS = {"2m": scenes.config2, "8m": scenes.config3, "32k": scenes.config1, "32m": scenes.config5}
 
 
 def main():

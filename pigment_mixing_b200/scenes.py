@@ -131,6 +131,35 @@ def config3(seed: int = 0) -> dict:
     return four_block_scene(1.0 / 384, (64, 64, 64), seed, 2000)
 
 
+def six_block_scene(dx: float, block_cells=(87, 87, 87), seed: int = 0, steps: int = 4000) -> dict:
+    """3 x 2 blocks (x by z) of six pigments on the floor and a box knife making four
+    back-and-forth strokes through them along z."""
+    rng = np.random.default_rng(seed)
+    bc = np.asarray(block_cells, np.int64)
+    size = bc * dx
+    x0 = 0.5 - 1.5 * size[0]
+    z0 = 0.5 - size[2]
+    xs, lats = [], []
+    for k, (ix, iz) in enumerate([(i, j) for j in range(2) for i in range(3)]):
+        blk = jittered_block([x0 + ix * size[0], 0.0, z0 + iz * size[2]], bc, dx, rng)
+        xs.append(blk)
+        lats.append(np.tile(MIXBOX_LATENTS[RGB_SEEDS[k]], (len(blk), 1)))
+    sc = two_block_scene(dx, block_cells, seed, steps)
+    sc["x"] = np.concatenate(xs)
+    sc["latent"] = np.concatenate(lats).astype(np.float32)
+    half = [0.2, 0.1, 0.005]
+    path = knife_path(rng, 0.5, half[1] + 0.5 * dx, z0 - 0.05, z0 + 2 * size[2] + 0.05, segments=8)
+    sc["objects"] = [sc["objects"][0], ("box_knife", dict(bc=2, friction=0.3, half=half, waypoints=path, speed=0.5))]
+    sc["name"] = f"six_blocks_dx{1.0 / dx:.0f}"
+    return sc
+
+
+def config5(seed: int = 0) -> dict:
+    """512^3 grid, dx = 1/512, six 87^3-cell blocks in a 3 x 2 arrangement: 31,608,144 particles,
+    a knife making four back-and-forth strokes, 4000 steps."""
+    return six_block_scene(1.0 / 512, (87, 87, 87), seed, 4000)
+
+
 def palette_scene(n_particles: int, grid_res: int, pair=(0, 1), yield_pa: float = 100.0, seed: int = 0,
                   steps: int = 500) -> dict:
     """One palette scene of the batched workload: the two-block recipe at dx = 1/grid_res with
