@@ -207,6 +207,25 @@ PM_API const char* pm_kernel_name(pm_sim* sim, int index);
  * step (pm_get_param "kernels_per_step"). */
 PM_API pm_status pm_profile_steps(pm_sim* sim, uint32_t nsteps, float* kernel_ms, uint32_t n_kernels);
 
+/* ---- output files and checkpoints -------------------------------------------------------------
+ * Simulation::saveParticleData(extra) (save_data.cpp:7-166): binary little-endian PLY
+ * `<directory><name>/particles_f<extra><frame>.ply` with float32 vertex properties x y z vx vy vz
+ * p q Je, plus eps_pl_vol eps_pl_dev delta_gamma when a plastic model is set (p = -tr(tau)/3,
+ * q = q_prefac |dev tau|, Je = det F, tau the Kirchhoff stress of F), and `last_written.txt` with the
+ * frame.  <name> is the pm_initialize_basic name; the directory must exist (as in the reference). */
+PM_API pm_status pm_save_particle_data(pm_sim* sim, const char* directory, const char* extra);
+/* Simulation::saveGridData(extra) (save_data.cpp:168-254): `<directory><name>/grid_f<extra><frame>.ply`
+ * with x y z vx vy vz mass for every node of the step's grid box (v: the MUSL velocity). */
+PM_API pm_status pm_save_grid_data(pm_sim* sim, const char* directory, const char* extra);
+/* Simulation::saveInfo() (save_data.cpp:347-356): `<directory><name>/info.txt`. */
+PM_API pm_status pm_save_info(pm_sim* sim, const char* directory);
+/* Checkpoints (no reference counterpart): the full particle state (all fields, original order,
+ * active flags) and the device control block (time, dt, step, frame, object poses, grid reference
+ * box).  Load into a simulation set up like the saved one and prepared; the run then continues as
+ * the saved one would.  A checkpoint is tied to the library build that wrote it. */
+PM_API pm_status pm_save_checkpoint(pm_sim* sim, const char* path);
+PM_API pm_status pm_load_checkpoint(pm_sim* sim, const char* path);
+
 /* ---- batched scenes --------------------------------------------------------------------------
  * No counterpart in the reference, which runs one Simulation per process
  * (R/src/mpm/MPMIntegrationSim.cpp:16-38 creates one).  A batch steps many independent, prepared

@@ -58,6 +58,11 @@ SIGNATURES = {
     "pm_mlp_loss_grad": [_fp, _fp, _fp, C.c_uint32, _fp, _fp],
     "pm_mlp_infer": [_fp, _fp, C.c_uint32, _fp],
     "pm_p2g_noalloc": [_vp] * 5 + [C.c_uint32, C.c_double, C.c_double, _dp, C.POINTER(C.c_int32)] + [_vp] * 5 + [_up],
+    "pm_save_particle_data": [_vp, C.c_char_p, C.c_char_p],
+    "pm_save_grid_data": [_vp, C.c_char_p, C.c_char_p],
+    "pm_save_info": [_vp, C.c_char_p],
+    "pm_save_checkpoint": [_vp, C.c_char_p],
+    "pm_load_checkpoint": [_vp, C.c_char_p],
     "pm_batch_create": [C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(C.c_void_p)],
     "pm_batch_destroy": [_vp],
     "pm_batch_step": [_vp, C.c_uint32],

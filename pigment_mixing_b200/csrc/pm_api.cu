@@ -1709,3 +1709,183 @@ pm_status pm_batch_autotune(pm_batch* b, uint32_t trial_rounds, pm_batch_tuning*
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// output files (save_data.cpp) and checkpoints
+// ------------------------------------------------------------------------------------------
+namespace {
+
+// Binary little-endian PLY with float32 vertex properties: the format the reference writes through
+// tinyply (save_data.cpp:36-162, `file.write(out, true)`).
+pm_status write_ply(const std::string& path, const std::vector<std::string>& props, const float* rows, size_t n) {
+  std::ofstream f(path, std::ios::binary);
+  if (!f) return fail(PM_ERR_IO, "cannot open " + path);
+  f << "ply\nformat binary_little_endian 1.0\nelement vertex " << n << "\n";
+  for (const std::string& p : props) f << "property float " << p << "\n";
+  f << "end_header\n";
+  f.write(reinterpret_cast<const char*>(rows), (std::streamsize)(sizeof(float) * props.size() * n));
+  if (!f) return fail(PM_ERR_IO, "write failed: " + path);
+  return PM_OK;
+}
+
+pm_status write_text(const std::string& path, const std::string& text) {
+  std::ofstream f(path);
+  if (!f) return fail(PM_ERR_IO, "cannot open " + path);
+  f << text;
+  return f ? PM_OK : fail(PM_ERR_IO, "write failed: " + path);
+}
+
+constexpr char kCkptMagic[8] = {'P', 'M', 'C', 'K', 'P', 'T', '0', '1'};
+struct CkptHeader {
+  char magic[8];
+  uint32_t version, np, nfields, ctrl_bytes;
+};
+
+}  // namespace
+
+extern "C" {
+
+pm_status pm_save_particle_data(pm_sim* sim, const char* directory, const char* extra) {
+  if (!sim || !directory) return fail(PM_ERR_INVALID, "NULL argument");
+  if (!sim->prepared) return fail(PM_ERR_STATE, "call pm_prepare first");
+  CK(cudaSetDevice(sim->device));
+  pm_status s = sim->sync_ctrl();
+  if (s != PM_OK) return s;
+  const uint32_t n = sim->np;
+  Params p = sim->P;
+  launch_ply_particles(p, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], sim->d_unperm, sim->stream);
+  CK(cudaGetLastError());
+  std::vector<float> rows((size_t)n * kPlyFields);
+  CK(cudaMemcpyAsync(rows.data(), sim->d_unperm, rows.size() * sizeof(float), cudaMemcpyDeviceToHost, sim->stream));
+  CK(cudaStreamSynchronize(sim->stream));
+  std::vector<std::string> props = {"x", "y", "z", "vx", "vy", "vz", "p", "q", "Je"};
+  if (sim->hp.plastic_model != PM_NO_PLASTICITY) {
+    props.insert(props.end(), {"eps_pl_vol", "eps_pl_dev", "delta_gamma"});
+  } else {  // compact the rows to the 9 written properties
+    for (size_t r = 0; r < n; ++r)
+      for (int k = 0; k < 9; ++k) rows[r * 9 + k] = rows[r * kPlyFields + k];
+  }
+  const std::string dir = std::string(directory) + sim->name;
+  const std::string frame = std::to_string(sim->h_ctrl->frame);
+  s = write_ply(dir + "/particles_f" + (extra ? extra : "") + frame + ".ply", props, rows.data(), n);
+  if (s != PM_OK) return s;
+  return write_text(dir + "/last_written.txt", frame + "\n");
+}
+
+pm_status pm_save_grid_data(pm_sim* sim, const char* directory, const char* extra) {
+  if (!sim || !directory) return fail(PM_ERR_INVALID, "NULL argument");
+  double origin[3];
+  uint32_t dims[3];
+  pm_status s = pm_get_grid(sim, origin, dims, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+  if (s != PM_OK) return s;
+  const size_t nn = (size_t)dims[0] * dims[1] * dims[2];
+  std::vector<float> mass(nn), v(3 * nn);
+  // the reference's grid.v after a step is the MUSL velocity (USL: the updated velocity)
+  if (sim->hp.use_musl) s = pm_get_grid(sim, origin, dims, mass.data(), nullptr, v.data(), nullptr, nullptr, nullptr);
+  else s = pm_get_grid(sim, origin, dims, mass.data(), v.data(), nullptr, nullptr, nullptr, nullptr);
+  if (s != PM_OK) return s;
+  std::vector<float> rows(7 * nn);
+  const double dx = sim->hp.dx;
+  for (uint32_t i = 0; i < dims[0]; ++i)
+    for (uint32_t j = 0; j < dims[1]; ++j)
+      for (uint32_t k = 0; k < dims[2]; ++k) {
+        const size_t l = ((size_t)i * dims[1] + j) * dims[2] + k;
+        float* r = &rows[7 * l];
+        r[0] = (float)(origin[0] + i * dx); r[1] = (float)(origin[1] + j * dx); r[2] = (float)(origin[2] + k * dx);
+        r[3] = v[3 * l]; r[4] = v[3 * l + 1]; r[5] = v[3 * l + 2];
+        r[6] = mass[l];
+      }
+  const std::string dir = std::string(directory) + sim->name;
+  return write_ply(dir + "/grid_f" + (extra ? extra : "") + std::to_string(sim->h_ctrl->frame) + ".ply",
+                   {"x", "y", "z", "vx", "vy", "vz", "mass"}, rows.data(), nn);
+}
+
+pm_status pm_save_info(pm_sim* sim, const char* directory) {
+  if (!sim || !directory) return fail(PM_ERR_INVALID, "NULL argument");
+  std::ostringstream t;  // save_data.cpp:347-356, one value per line
+  t << sim->hp.end_frame << "\n" << sim->hp.fps << "\n" << sim->hp.dx << "\n" << sim->np << "\n"
+    << sim->hp.particle_volume << "\n";
+  return write_text(std::string(directory) + sim->name + "/info.txt", t.str());
+}
+
+pm_status pm_save_checkpoint(pm_sim* sim, const char* path) {
+  if (!sim || !path) return fail(PM_ERR_INVALID, "NULL argument");
+  if (!sim->prepared) return fail(PM_ERR_STATE, "call pm_prepare first");
+  CK(cudaSetDevice(sim->device));
+  pm_status s = sim->sync_ctrl();
+  if (s != PM_OK) return s;
+  const uint32_t n = sim->np;
+  Params p = sim->P;
+  launch_unpermute(p, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], sim->d_unperm, sim->d_active, sim->stream);
+  CK(cudaGetLastError());
+  std::vector<float> fields((size_t)n * F_COUNT);
+  std::vector<uint8_t> active(n);
+  CK(cudaMemcpyAsync(fields.data(), sim->d_unperm, fields.size() * sizeof(float), cudaMemcpyDeviceToHost, sim->stream));
+  CK(cudaMemcpyAsync(active.data(), sim->d_active, n, cudaMemcpyDeviceToHost, sim->stream));
+  CK(cudaStreamSynchronize(sim->stream));
+  std::ofstream f(path, std::ios::binary);
+  if (!f) return fail(PM_ERR_IO, std::string("cannot open ") + path);
+  CkptHeader h{};
+  std::memcpy(h.magic, kCkptMagic, 8);
+  h.version = 1;
+  h.np = n;
+  h.nfields = F_COUNT;
+  h.ctrl_bytes = (uint32_t)sizeof(Ctrl);
+  f.write(reinterpret_cast<const char*>(&h), sizeof(h));
+  f.write(reinterpret_cast<const char*>(fields.data()), (std::streamsize)(fields.size() * sizeof(float)));
+  f.write(reinterpret_cast<const char*>(active.data()), (std::streamsize)active.size());
+  f.write(reinterpret_cast<const char*>(sim->h_ctrl), sizeof(Ctrl));
+  return f ? PM_OK : fail(PM_ERR_IO, std::string("write failed: ") + path);
+}
+
+pm_status pm_load_checkpoint(pm_sim* sim, const char* path) {
+  if (!sim || !path) return fail(PM_ERR_INVALID, "NULL argument");
+  if (!sim->prepared) return fail(PM_ERR_STATE, "set up the same scene and call pm_prepare before loading");
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return fail(PM_ERR_IO, std::string("cannot open ") + path);
+  CkptHeader h{};
+  f.read(reinterpret_cast<char*>(&h), sizeof(h));
+  if (!f || std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1)
+    return fail(PM_ERR_IO, "not a checkpoint of this library");
+  if (h.nfields != F_COUNT || h.ctrl_bytes != sizeof(Ctrl))
+    return fail(PM_ERR_UNSUPPORTED, "checkpoint written by a different build of the library");
+  if (h.np != sim->np) return fail(PM_ERR_INVALID, "checkpoint particle count differs from the scene's");
+  std::vector<float> fields((size_t)h.np * F_COUNT);
+  std::vector<uint8_t> active(h.np);
+  Ctrl c{};
+  f.read(reinterpret_cast<char*>(fields.data()), (std::streamsize)(fields.size() * sizeof(float)));
+  f.read(reinterpret_cast<char*>(active.data()), (std::streamsize)active.size());
+  f.read(reinterpret_cast<char*>(&c), sizeof(Ctrl));
+  if (!f) return fail(PM_ERR_IO, "checkpoint is truncated");
+  CK(cudaSetDevice(sim->device));
+  CK(cudaStreamSynchronize(sim->stream));
+  float* d_in = nullptr;
+  uint8_t* d_act = nullptr;
+  CK(cudaMalloc(&d_in, fields.size() * sizeof(float)));
+  if (cudaMalloc(&d_act, std::max<size_t>(active.size(), 1)) != cudaSuccess) {
+    cudaFree(d_in);
+    return fail(PM_ERR_CUDA, "allocation for the checkpoint failed");
+  }
+  cudaMemcpy(d_in, fields.data(), fields.size() * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(d_act, active.data(), active.size(), cudaMemcpyHostToDevice);
+  sim->drop_graphs();
+  sim->cur = 0;
+  Params p = sim->P;
+  launch_load_fields(p, d_in, d_act, sim->d_pbuf[0], sim->d_meta[0], sim->stream);
+  const cudaError_t e = cudaStreamSynchronize(sim->stream);
+  cudaFree(d_in);
+  cudaFree(d_act);
+  if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("checkpoint upload: ") + cudaGetErrorString(e));
+  // the control block as saved (time, dt, step, frame, object poses, reference boxes, reductions)
+  c.halt = 0;
+  c.idle = 0;
+  c.target_step = 0;
+  *sim->h_ctrl = c;
+  sim->host_step = c.step;
+  pm_status s = sim->push_ctrl();
+  if (s != PM_OK) return s;
+  sim->fill_params();
+  return PM_OK;
+}
+
+}  // extern "C"

@@ -2000,6 +2000,24 @@ __global__ void k_upload(Params P, const float* x, const float* lat, const float
   }
 }
 
+// Inverse of k_unpermute for checkpoints: particle pid's fields from the grouped host layout
+// (group base * np + pid * group width + component) into slot pid of the SoA buffer.
+__global__ void k_load_fields(Params P, const float* in, const uint8_t* active, float* pbuf, uint32_t* meta) {
+  const int S = P.np_stride, np = P.np;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < S; p += gridDim.x * blockDim.x) {
+    if (p >= np) {
+      for (int f = 0; f < F_COUNT; ++f) pbuf[f * S + p] = 0.f;
+      meta[p] = kInactiveBit;
+      continue;
+    }
+    for (int f = 0; f < F_COUNT; ++f) {  // a group's base is the index of its first field
+      const int g = c_group_base[f], w = c_group_width[f];
+      pbuf[f * S + p] = in[(size_t)g * np + (size_t)p * w + (f - g)];
+    }
+    meta[p] = (uint32_t)p | (active[p] ? 0u : kInactiveBit);
+  }
+}
+
 // Diagnostics: mass, momentum, mass-weighted latent sums (double atomics per block).
 __global__ void __launch_bounds__(kThreads) k_stats(Params P, const float* pcur, const uint32_t* meta, double* acc) {
   const int S = P.np_stride;
@@ -2171,6 +2189,41 @@ void launch_unpermute(const Params& P, const float* pcur, const uint32_t* meta, 
   const int sms = g_num_sms > 0 ? g_num_sms : 148;
   k_unpermute<<<sms * 4, 256, 0, s>>>(P, pcur, meta, out, active);
 }
+// Per particle, in original order: the reference's PLY vertex row (save_data.cpp:7-166) -- x, v,
+// pressure p = -tr(tau)/3, deviatoric stress q = q_prefac |tau + p I|, Je = det F, eps_pl_vol,
+// eps_pl_dev, delta_gamma -- from the cached Kirchhoff stress tau of the current F.
+__global__ void k_ply_particles(Params P, const float* pcur, const uint32_t* meta, float* out) {
+  const int S = P.np_stride, np = P.np;
+  const float q_prefac = (float)(1.0 / P.d_prefac);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    const uint32_t pid = meta[i] & ~kInactiveBit;
+    if (pid >= (uint32_t)np) continue;
+    float* o = out + (size_t)pid * kPlyFields;
+    for (int k = 0; k < 3; ++k) { o[k] = pcur[(F_X + k) * S + i]; o[3 + k] = pcur[(F_V + k) * S + i]; }
+    float t[6], F[9];
+    for (int k = 0; k < 6; ++k) t[k] = pcur[(F_TAU + k) * S + i];
+    for (int k = 0; k < 9; ++k) F[k] = pcur[(F_F + k) * S + i];
+    const float pr = -(t[0] + t[1] + t[2]) / 3.f;
+    const float d0 = t[0] + pr, d1 = t[1] + pr, d2 = t[2] + pr;
+    const float dd = d0 * d0 + d1 * d1 + d2 * d2 + 2.f * (t[3] * t[3] + t[4] * t[4] + t[5] * t[5]);
+    o[6] = pr;
+    o[7] = q_prefac * sqrtf(dd);
+    o[8] = F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) + F[2] * (F[3] * F[7] - F[4] * F[6]);
+    o[9] = pcur[F_EPV * S + i];
+    o[10] = pcur[F_EPD * S + i];
+    o[11] = pcur[F_DG * S + i];
+  }
+}
+void launch_load_fields(const Params& P, const float* in, const uint8_t* active, float* pbuf, uint32_t* meta,
+                        cudaStream_t s) {
+  const int sms = g_num_sms > 0 ? g_num_sms : 148;
+  k_load_fields<<<sms * 4, 256, 0, s>>>(P, in, active, pbuf, meta);
+}
+void launch_ply_particles(const Params& P, const float* pcur, const uint32_t* meta, float* out, cudaStream_t s) {
+  const int sms = g_num_sms > 0 ? g_num_sms : 148;
+  k_ply_particles<<<sms * 4, 256, 0, s>>>(P, pcur, meta, out);
+}
+
 void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, double* acc, cudaStream_t s) {
   const int sms = g_num_sms > 0 ? g_num_sms : 148;
   k_stats<<<sms * 2, kThreads, 0, s>>>(P, pcur, meta, acc);

@@ -21,6 +21,12 @@ void launch_unpermute(const Params& P, const float* pcur, const uint32_t* meta, 
 void launch_upload(const Params& P, const float* x, const float* lat, const float* v, float* pbuf, uint32_t* meta,
                    cudaStream_t s);
 void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, double* acc, cudaStream_t s);
+// The reference's particle PLY row: x y z vx vy vz p q Je eps_pl_vol eps_pl_dev delta_gamma.
+constexpr int kPlyFields = 12;
+void launch_ply_particles(const Params& P, const float* pcur, const uint32_t* meta, float* out, cudaStream_t s);
+// Checkpoint load: grouped host layout of pm_get_particles' unpermute (all F_COUNT fields) -> SoA.
+void launch_load_fields(const Params& P, const float* in, const uint8_t* active, float* pbuf, uint32_t* meta,
+                        cudaStream_t s);
 
 // Batched scenes: the SceneDev table and, per kernel class, device tables of CTA offsets
 // (ns + 1 entries; scene s owns CTAs [off[s], off[s+1])) with their totals.

@@ -253,6 +253,25 @@ class Simulation:
         call("pm_profile_steps", self._h, int(nsteps), _fp(ms), k)
         return {lib().pm_kernel_name(self._h, i).decode(): float(ms[i]) for i in range(k)}
 
+    # ---- output files (save_data.cpp) and checkpoints ----------------------------------------
+    def saveParticleData(self, directory: str, extra: str = "") -> None:
+        """Binary PLY `<directory><name>/particles_f<extra><frame>.ply` (save_data.cpp:7-166)."""
+        call("pm_save_particle_data", self._h, directory.encode(), extra.encode())
+
+    def saveGridData(self, directory: str, extra: str = "") -> None:
+        """Binary PLY `<directory><name>/grid_f<extra><frame>.ply` (save_data.cpp:168-254)."""
+        call("pm_save_grid_data", self._h, directory.encode(), extra.encode())
+
+    def saveInfo(self, directory: str) -> None:
+        call("pm_save_info", self._h, directory.encode())
+
+    def saveCheckpoint(self, path: str) -> None:
+        call("pm_save_checkpoint", self._h, path.encode())
+
+    def loadCheckpoint(self, path: str) -> None:
+        """Restore a checkpoint into this (identically set up, prepared) simulation."""
+        call("pm_load_checkpoint", self._h, path.encode())
+
     def errorFlags(self, clear: bool = False) -> int:
         f = C.c_uint32()
         call("pm_get_error_flags", self._h, C.byref(f), int(clear))
