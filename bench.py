@@ -121,7 +121,9 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def _dist():
+def _dist(backend: str = "nccl"):
+    """(process group or None, rank, world size, local rank) from the torchrun environment.
+    Replicas: the group carries only the barrier and the max-over-ranks of the timings."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws <= 1:
         return None, 0, 1, 0
@@ -129,15 +131,20 @@ def _dist():
     from datetime import timedelta
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=None)
+    dist.init_process_group(backend, timeout=timedelta(seconds=600))
     return dist, rank, ws, local
+
+
+def _coll_device(dist, device):
+    """Where collective tensors live: the GPU for NCCL, the host for gloo."""
+    return device if dist is not None and dist.get_backend() == "nccl" else "cpu"
 
 
 def _max_over_ranks(dist, x: float, device) -> float:
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device=device)
+    t = torch.tensor([x], dtype=torch.float64, device=_coll_device(dist, device))
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -145,9 +152,17 @@ def _max_over_ranks(dist, x: float, device) -> float:
 def _barrier(dist, device):
     if dist is not None:
         import torch
-        t = torch.zeros(1, device=device)
+        t = torch.zeros(1, device=_coll_device(dist, device))
         dist.all_reduce(t)
-        torch.cuda.synchronize(device)
+        if t.is_cuda:
+            torch.cuda.synchronize(device)
+
+
+def replica_throughput(dist, ws: int, units_per_rank: int, steps: int, ms_local: float, device) -> tuple:
+    """Whole-job throughput of N independent replicas: every rank processed units_per_rank x steps
+    units; the job took the slowest rank's time.  Returns (max ms over ranks, units per second)."""
+    ms = _max_over_ranks(dist, ms_local, device)
+    return ms, ws * units_per_rank * steps / (ms / 1e3)
 
 
 def cpu_baseline(scene, budget_s: float = 25.0, max_steps: int = 20):
@@ -312,8 +327,7 @@ def run_ours(args):
     ref = sim.getParticles(fields=("x", "latent"))
     x_ref, lat_ref = ref.x, ref.latent
     newton_plain = _newton_per_solve(sim, 4)
-    ms_max = _max_over_ranks(dist, ms, device)
-    value = ws * npart * args.steps / (ms_max / 1e3)
+    ms_max, value = replica_throughput(dist, ws, npart, args.steps, ms, device)
     # -------- per-kernel times (CUDA events on the same stream, separate steps) --------
     g = sim.grid()
     active_nodes = int((g["mass"] > 0).sum())
