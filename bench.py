@@ -350,6 +350,9 @@ def run_ours(args):
     sur = None
     if not args.no_surrogate:
         sur = _surrogate_leg(scene, args, device, dist, ws, value, x_ref, lat_ref, newton_plain)
+    splat = None
+    if not args.no_splat:
+        splat = _splat_leg(scene, args, device, dist, rank == 0 and ws == 1 and not args.no_cpu)
     batch = None
     if not args.no_batch:
         batch = _batch_leg(args, device, dist, ws)
@@ -365,6 +368,8 @@ def run_ours(args):
         line["surrogate"] = sur
     if batch is not None:
         line["batch"] = batch
+    if splat is not None:
+        line["splat"] = splat
     if args.drift_steps > 0:
         line["drift"] = drift(scene, args.drift_steps, device)
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -533,6 +538,47 @@ def _batch_leg(args, device, dist, ws):
                         "random 3-segment knife path, VMVisc, MUSL, APIC, plain return map"}
 
 
+def _splat_leg(scene, args, device, dist, with_cpu: bool):
+    """Headless pigment volume splat (the renderer's two-pass bilateral splat) of the workload
+    after its warm-up steps: device time of pm_splat_pigments into a device buffer; beside it the
+    numpy restatement (the checker) on a sample of the particles."""
+    import torch
+    from pigment_mixing_b200 import Simulation, scenes
+    g = Simulation(device)
+    scenes.apply(scene, g)
+    g.prepareSimulation()
+    g.advance(args.warmup)
+    vox0, origin, vs = g.splatPigments(0.5, 0.2)
+    out = torch.empty(vox0.shape, dtype=torch.float32, device=f"cuda:{device}")
+    stream = torch.cuda.ExternalStream(g.stream(), device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g.splatPigments(0.5, 0.2, out=out)  # warm-up
+    torch.cuda.synchronize(device)
+    reps = 5
+    e0.record(stream)
+    for _ in range(reps):
+        g.splatPigments(0.5, 0.2, out=out)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = _max_over_ranks(dist, e0.elapsed_time(e1) / reps, device)
+    n = len(scene["x"])
+    res = {"particles": n, "voxels": int(np.prod(vox0.shape[:3])), "voxel_size": vs, "ms": ms,
+           "particles_per_s": n / (ms / 1e3), "sigma_spatial": 0.5, "sigma_color": 0.2,
+           "includes": "allocation of the two 8-float voxel grids, both passes and normalisations; no host copy"}
+    if with_cpu:
+        from oracle import splat_ref
+        st = g.getParticles(fields=("x", "latent"))
+        lo, hi = g.getGridBoundaries()
+        k = min(n, 50000)
+        t0 = time.perf_counter()
+        splat_ref.splat(st.x[:k], st.latent[:k], lo, hi, scene["params"]["dx"], 0.5, 0.2)
+        el = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": k / el, "unit": "particles/s", "cores": 1, "kind": "port",
+                               "sample": f"first {k} particles, numpy restatement of both passes"}
+    g.close()
+    return res
+
+
 def _e2e(scene, args, device, dist, ws):
     import torch
     from pigment_mixing_b200 import Simulation, scenes
@@ -589,6 +635,7 @@ def main():
     ap.add_argument("--log-steps", type=int, default=20, help="plain steps logged for surrogate training")
     ap.add_argument("--train-epochs", type=int, default=30)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenes leg")
+    ap.add_argument("--no-splat", action="store_true", help="skip the pigment-splat leg")
     ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=50, help="timed rounds of the batched leg")
     ap.add_argument("--drift-steps", type=int, default=1000,

@@ -74,9 +74,11 @@ PM_API pm_status pm_initialize_basic(pm_sim* sim, const char* name);
  * "min_dt", "dx", "particle_mass", "particle_volume", "plastic_model", "use_pradhana", "use_musl",
  * "use_particle_boundaries", "q_max", "q_min", "p_min", "M", "q_cohesion", "perzyna_exp",
  * "perzyna_visc", "xi", "q_prefac", "pigment_D_max", "pigment_D_edge0", "pigment_D_edge1",
- * "start_boost_time", "end_boost_time", "boost_factor", "frame", "auto_frame".
+ * "start_boost_time", "end_boost_time", "boost_factor", "frame", "auto_frame"; and (no reference
+ * counterpart) "surrogate_fallback_plain", "sample_log_every".
  * Read-only extras for pm_get_param: "time", "dt", "step", "Np", "mu", "lambda", "K", "dt_max",
- * "frame_dt", "final_time", "n_active", "plastic_count", "grid_nodes", "kernels_per_step". */
+ * "frame_dt", "final_time", "n_active", "plastic_count", "grid_nodes", "kernels_per_step",
+ * "regrowths", "regrow_ms", "grid_capacity_nodes". */
 PM_API pm_status pm_set_param(pm_sim* sim, const char* name, double value);
 PM_API pm_status pm_get_param(pm_sim* sim, const char* name, double* value);
 /* Vector fields: "gravity", "particle_boundary_min", "particle_boundary_max", "grid_reference_point". */
@@ -225,6 +227,18 @@ PM_API pm_status pm_save_info(pm_sim* sim, const char* directory);
  * the saved one would.  A checkpoint is tied to the library build that wrote it. */
 PM_API pm_status pm_save_checkpoint(pm_sim* sim, const char* path);
 PM_API pm_status pm_load_checkpoint(pm_sim* sim, const char* path);
+
+/* ---- headless pigment splat --------------------------------------------------------------------
+ * BinaryDensityGrid::fillRenderGrid (raytracing/src/raymarch/BinaryDensityGrid.cpp:153-296) without
+ * the GL upload: the two-pass anisotropic bilateral splat of the particle latents onto the pigment
+ * grid, whose voxels are a quarter of the density voxel (the support radius 2 dx,
+ * MPMIntegrationSim.cpp:96-98) over the grid boundaries (AABBc.cpp:10-25).  voxels[dims z][y][x][8]
+ * receives latent 7 + weight per voxel; NULL only fills dims, origin and voxel_size.  G: per-particle
+ * 3x3 anisotropy matrices (row-major, original particle order) or NULL for the isotropic I / h the
+ * reference uses for sparse neighbourhoods.  device_ptrs: G and voxels are device pointers. */
+PM_API pm_status pm_splat_pigments(pm_sim* sim, const float* G, int device_ptrs, float sigma_spatial,
+                                   float sigma_color, float* voxels, uint32_t dims[3], double origin[3],
+                                   double* voxel_size);
 
 /* ---- batched scenes --------------------------------------------------------------------------
  * No counterpart in the reference, which runs one Simulation per process

@@ -1889,3 +1889,72 @@ pm_status pm_load_checkpoint(pm_sim* sim, const char* path) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// headless pigment splat (BinaryDensityGrid::fillRenderGrid)
+// ------------------------------------------------------------------------------------------
+extern "C" {
+
+pm_status pm_splat_pigments(pm_sim* sim, const float* G, int device_ptrs, float sigma_spatial, float sigma_color,
+                            float* voxels, uint32_t dims[3], double origin[3], double* voxel_size) {
+  if (!sim || !dims) return fail(PM_ERR_INVALID, "NULL argument");
+  if (!sim->prepared) return fail(PM_ERR_STATE, "call pm_prepare first");
+  CK(cudaSetDevice(sim->device));
+  pm_status s = sim->sync_ctrl();
+  if (s != PM_OK) return s;
+  // AABBc::fixedAABB (AABBc.cpp:10-25): density voxels of the support radius 2 dx
+  // (MPMIntegrationSim.cpp:96-98) over the grid boundaries; the pigment grid is 4x finer
+  const float h = (float)(2.0 * sim->hp.dx);
+  SplatGeom g{};
+  for (int d = 0; d < 3; ++d) {
+    const float mn = (float)sim->h_ctrl->low[d], mx = (float)sim->h_ctrl->high[d];
+    const float start = std::floor(mn / h) * h;
+    const int cells = (int)std::ceil((mx - mn) / h) + 1;
+    g.start[d] = start;
+    g.dims[d] = 4 * cells;
+    dims[d] = (uint32_t)g.dims[d];
+    if (origin) origin[d] = start;
+  }
+  g.v4 = h / 4.0f;
+  if (voxel_size) *voxel_size = g.v4;
+  if (!voxels) return PM_OK;  // size query
+  // BinaryDensityGrid.cpp:162-170: sigmas floored at 0.001, search extent 3 h sigma_s, at most 12
+  const float ss = std::max(sigma_spatial, 0.001f), sc = std::max(sigma_color, 0.001f);
+  g.ext = std::min(12, (int)std::ceil(h * 3.0f * ss / g.v4));
+  g.sig_s2 = ss * ss;
+  g.sig_c2 = sc * sc;
+  g.inv_h = 1.0f / h;
+  const size_t nvox = (size_t)g.dims[0] * g.dims[1] * g.dims[2];
+  const size_t bytes = nvox * 8 * sizeof(float);
+  float* d_tmp = nullptr;
+  float* d_out = device_ptrs ? voxels : nullptr;
+  float* d_G = nullptr;
+  auto release = [&]() {
+    if (d_tmp) cudaFree(d_tmp);
+    if (!device_ptrs && d_out) cudaFree(d_out);
+    if (!device_ptrs && d_G) cudaFree(d_G);
+  };
+  if (cudaMalloc(&d_tmp, bytes) != cudaSuccess || (!device_ptrs && cudaMalloc(&d_out, bytes) != cudaSuccess)) {
+    release();
+    return fail(PM_ERR_CUDA, "allocation of the splat grids failed");
+  }
+  const float* Gd = G;
+  if (G && !device_ptrs) {
+    if (cudaMalloc(&d_G, (size_t)sim->np * 9 * sizeof(float)) != cudaSuccess) {
+      release();
+      return fail(PM_ERR_CUDA, "allocation of the anisotropy matrices failed");
+    }
+    cudaMemcpy(d_G, G, (size_t)sim->np * 9 * sizeof(float), cudaMemcpyHostToDevice);
+    Gd = d_G;
+  }
+  Params p = sim->P;
+  cudaError_t e = launch_splat(p, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], Gd, g, d_tmp, d_out, sim->stream);
+  if (e == cudaSuccess && !device_ptrs)
+    e = cudaMemcpyAsync(voxels, d_out, bytes, cudaMemcpyDeviceToHost, sim->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(sim->stream);
+  release();
+  if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("pigment splat: ") + cudaGetErrorString(e));
+  return PM_OK;
+}
+
+}  // extern "C"

@@ -24,6 +24,18 @@ void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, doub
 // The reference's particle PLY row: x y z vx vy vz p q Je eps_pl_vol eps_pl_dev delta_gamma.
 constexpr int kPlyFields = 12;
 void launch_ply_particles(const Params& P, const float* pcur, const uint32_t* meta, float* out, cudaStream_t s);
+// Pigment splat geometry (BinaryDensityGrid::fillRenderGrid): fine-voxel origin and size, voxel
+// counts, search half-extent in voxels, squared spatial and colour sigmas, isotropic 1/h.
+struct SplatGeom {
+  float start[3];
+  float v4;
+  int dims[3];
+  int ext;
+  float sig_s2, sig_c2, inv_h;
+};
+// Two-pass splat into out[dims z][y][x][8] (latent 7 + weight); tmp: same size, pass-1 grid.
+cudaError_t launch_splat(const Params& P, const float* pcur, const uint32_t* meta, const float* G, const SplatGeom& g,
+                         float* tmp, float* out, cudaStream_t s);
 // Checkpoint load: grouped host layout of pm_get_particles' unpermute (all F_COUNT fields) -> SoA.
 void launch_load_fields(const Params& P, const float* in, const uint8_t* active, float* pbuf, uint32_t* meta,
                         cudaStream_t s);

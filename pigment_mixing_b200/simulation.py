@@ -265,6 +265,31 @@ class Simulation:
     def saveInfo(self, directory: str) -> None:
         call("pm_save_info", self._h, directory.encode())
 
+    def splatPigments(self, sigma_spatial: float = 0.5, sigma_color: float = 0.2, G=None, out=None):
+        """The renderer's pigment volume (BinaryDensityGrid::fillRenderGrid) without GL.  Returns
+        (voxels[z][y][x][8] float32: latent 7 + weight, origin[3], voxel size).  G: optional
+        per-particle 3x3 anisotropy matrices (n x 3 x 3, original order); out: optional device
+        tensor (torch, float32, contiguous) to fill in place instead of a host array."""
+        dims = np.zeros(3, np.uint32)
+        origin = np.zeros(3)
+        vs = C.c_double()
+        up = dims.ctypes.data_as(C.POINTER(C.c_uint32))
+        call("pm_splat_pigments", self._h, None, 0, sigma_spatial, sigma_color, None, up, _dp(origin), C.byref(vs))
+        shape = (int(dims[2]), int(dims[1]), int(dims[0]), 8)
+        if out is not None:
+            assert tuple(out.shape) == shape and out.is_cuda and out.is_contiguous()
+            gptr = None
+            if G is not None:
+                gptr = C.c_void_p(G.data_ptr())
+            call("pm_splat_pigments", self._h, gptr, 1, sigma_spatial, sigma_color, C.c_void_p(out.data_ptr()), up,
+                 _dp(origin), C.byref(vs))
+            return out, origin, vs.value
+        vox = np.zeros(shape, np.float32)
+        g = None if G is None else np.ascontiguousarray(G, np.float32).reshape(-1, 9)
+        call("pm_splat_pigments", self._h, None if g is None else g.ctypes.data_as(C.c_void_p), 0, sigma_spatial,
+             sigma_color, vox.ctypes.data_as(C.c_void_p), up, _dp(origin), C.byref(vs))
+        return vox, origin, vs.value
+
     def saveCheckpoint(self, path: str) -> None:
         call("pm_save_checkpoint", self._h, path.encode())
 
