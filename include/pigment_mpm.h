@@ -228,6 +228,13 @@ PM_API pm_status pm_save_info(pm_sim* sim, const char* directory);
 PM_API pm_status pm_save_checkpoint(pm_sim* sim, const char* path);
 PM_API pm_status pm_load_checkpoint(pm_sim* sim, const char* path);
 
+/* Mean latent of the active particles inside the vertical cylinder (x - cx)^2 + (z - cz)^2 <=
+ * radius^2 and their count: the sampling of MPMIntegrationSim::calculateAndPrintFinalColor
+ * (MPMIntegrationSim.cpp:48-90, centre (0, 0.1, 0) and radius 0.2 there), reduced on the device.
+ * The caller turns the mean latent into a colour with Mixbox's latent-to-RGB. */
+PM_API pm_status pm_sample_latent_cylinder(pm_sim* sim, double cx, double cz, double radius, double mean_latent[7],
+                                           uint32_t* count);
+
 /* ---- headless pigment splat --------------------------------------------------------------------
  * BinaryDensityGrid::fillRenderGrid (raytracing/src/raymarch/BinaryDensityGrid.cpp:153-296) without
  * the GL upload: the two-pass anisotropic bilateral splat of the particle latents onto the pigment

@@ -1076,6 +1076,28 @@ pm_status pm_get_stats(pm_sim* sim, double* total_mass, double momentum[3], doub
   return PM_OK;
 }
 
+pm_status pm_sample_latent_cylinder(pm_sim* sim, double cx, double cz, double radius, double mean_latent[7],
+                                    uint32_t* count) {
+  if (!sim || !mean_latent) return fail(PM_ERR_INVALID, "NULL argument");
+  for (int k = 0; k < 7; ++k) mean_latent[k] = 0.0;
+  if (count) *count = 0;
+  if (sim->np == 0) return PM_OK;
+  CK(cudaSetDevice(sim->device));
+  CK(cudaMemsetAsync(sim->d_stats, 0, 16 * sizeof(double), sim->stream));
+  Params p = sim->P;
+  p.np = (int)sim->np;
+  p.np_stride = sim->np_stride;
+  launch_stats(p, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], sim->d_stats, sim->stream, 1, (float)cx, (float)cz,
+               (float)(radius * radius));
+  CK(cudaGetLastError());
+  double h[16];
+  CK(cudaMemcpyAsync(h, sim->d_stats, sizeof(h), cudaMemcpyDeviceToHost, sim->stream));
+  CK(cudaStreamSynchronize(sim->stream));
+  if (h[0] > 0) for (int k = 0; k < 7; ++k) mean_latent[k] = h[4 + k] / h[0];
+  if (count) *count = (uint32_t)h[0];
+  return PM_OK;
+}
+
 pm_status pm_get_grid(pm_sim* sim, double origin[3], uint32_t dims[3], float* mass, float* v_update, float* v_musl,
                       float* flip, float* latent, float* shear) {
   if (!sim || !origin || !dims) return fail(PM_ERR_INVALID, "NULL argument");

@@ -2019,11 +2019,18 @@ __global__ void k_load_fields(Params P, const float* in, const uint8_t* active, 
 }
 
 // Diagnostics: mass, momentum, mass-weighted latent sums (double atomics per block).
-__global__ void __launch_bounds__(kThreads) k_stats(Params P, const float* pcur, const uint32_t* meta, double* acc) {
+// With cyl set, only particles inside the vertical cylinder (x - cx)^2 + (z - cz)^2 <= r2 count
+// (the sampling region of MPMIntegrationSim::calculateAndPrintFinalColor, MPMIntegrationSim.cpp:48-90).
+__global__ void __launch_bounds__(kThreads) k_stats(Params P, const float* pcur, const uint32_t* meta, double* acc,
+                                                    int cyl, float cx, float cz, float r2) {
   const int S = P.np_stride;
   double s[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.np; i += gridDim.x * blockDim.x) {
     if (meta[i] & kInactiveBit) continue;
+    if (cyl) {
+      const float ex = pcur[F_X * S + i] - cx, ez = pcur[(F_X + 2) * S + i] - cz;
+      if (ex * ex + ez * ez > r2) continue;
+    }
     s[0] += 1.0;
     for (int r = 0; r < 3; ++r) s[1 + r] += pcur[(F_V + r) * S + i];
     for (int k = 0; k < 7; ++k) s[4 + k] += pcur[(F_LAT + k) * S + i];
@@ -2224,9 +2231,10 @@ void launch_ply_particles(const Params& P, const float* pcur, const uint32_t* me
   k_ply_particles<<<sms * 4, 256, 0, s>>>(P, pcur, meta, out);
 }
 
-void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, double* acc, cudaStream_t s) {
+void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, double* acc, cudaStream_t s, int cyl,
+                  float cx, float cz, float r2) {
   const int sms = g_num_sms > 0 ? g_num_sms : 148;
-  k_stats<<<sms * 2, kThreads, 0, s>>>(P, pcur, meta, acc);
+  k_stats<<<sms * 4, kThreads, 0, s>>>(P, pcur, meta, acc, cyl, cx, cz, r2);
 }
 
 }  // namespace pm

@@ -20,7 +20,8 @@ void launch_unpermute(const Params& P, const float* pcur, const uint32_t* meta, 
                       cudaStream_t s);
 void launch_upload(const Params& P, const float* x, const float* lat, const float* v, float* pbuf, uint32_t* meta,
                    cudaStream_t s);
-void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, double* acc, cudaStream_t s);
+void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, double* acc, cudaStream_t s, int cyl = 0,
+                  float cx = 0.f, float cz = 0.f, float r2 = 0.f);
 // The reference's particle PLY row: x y z vx vy vz p q Je eps_pl_vol eps_pl_dev delta_gamma.
 constexpr int kPlyFields = 12;
 void launch_ply_particles(const Params& P, const float* pcur, const uint32_t* meta, float* out, cudaStream_t s);

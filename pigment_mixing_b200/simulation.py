@@ -265,6 +265,14 @@ class Simulation:
     def saveInfo(self, directory: str) -> None:
         call("pm_save_info", self._h, directory.encode())
 
+    def sampleLatentCylinder(self, cx: float = 0.0, cz: float = 0.0, radius: float = 0.2):
+        """(mean latent[7], count) of the active particles in a vertical cylinder (the final-colour
+        sampling of MPMIntegrationSim.cpp:48-90)."""
+        m = np.zeros(7)
+        n = C.c_uint32()
+        call("pm_sample_latent_cylinder", self._h, float(cx), float(cz), float(radius), _dp(m), C.byref(n))
+        return m, n.value
+
     def splatPigments(self, sigma_spatial: float = 0.5, sigma_color: float = 0.2, G=None, out=None):
         """The renderer's pigment volume (BinaryDensityGrid::fillRenderGrid) without GL.  Returns
         (voxels[z][y][x][8] float32: latent 7 + weight, origin[3], voxel size).  G: optional

@@ -49,3 +49,24 @@ def test_splat_matches_oracle(aniso):
     both = (w > 1e-3 * wr.max()) & (wr > 1e-3 * wr.max())
     assert both.sum() > 100
     assert np.abs(vox[both, :7] - ref[both, :7]).max() <= 2e-4
+
+
+@pytest.mark.gpu
+def test_cylinder_latent_sample_matches_particles():
+    """The final-colour sampling (MPMIntegrationSim.cpp:48-90) reduced on the device equals the
+    same average over the particles read back."""
+    from pigment_mixing_b200 import Simulation, scenes
+    sc = scenes.two_block_scene(1.0 / 32, (6, 6, 3), seed=8, steps=10)
+    g = Simulation(0)
+    scenes.apply(sc, g)
+    g.prepareSimulation()
+    g.advance(5)
+    st = g.getParticles(fields=("x", "latent", "active"))
+    for cx, cz, r in ((0.5, 0.5, 0.2), (0.45, 0.5, 0.05), (0.0, 0.1, 0.2)):
+        m, n = g.sampleLatentCylinder(cx, cz, r)
+        sel = (st.active > 0) & ((st.x[:, 0] - cx) ** 2 + (st.x[:, 2] - cz) ** 2 <= r * r)
+        assert n == int(sel.sum())
+        if n:
+            assert np.allclose(m, st.latent[sel].astype(np.float64).mean(0), atol=1e-6)
+        else:
+            assert np.all(m == 0)
