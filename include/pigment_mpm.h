@@ -235,6 +235,17 @@ PM_API pm_status pm_load_checkpoint(pm_sim* sim, const char* path);
 PM_API pm_status pm_sample_latent_cylinder(pm_sim* sim, double cx, double cz, double radius, double mean_latent[7],
                                            uint32_t* count);
 
+/* ---- scene builder -----------------------------------------------------------------------------
+ * sampleParticles (matter/src/sampling/sampling_particles.hpp:12-70) on the GPU: a Poisson-disk set
+ * of minimum distance `radius` in [0, Lx] x [0, Ly] x [0, Lz] (parallel dart throwing on a grid of
+ * cells of side radius / sqrt(3), 27 independent phases, `attempts` darts per cell and `passes`
+ * sweeps; deterministic for a seed), cropped like the reference (0 box, 1 cylinder of diameter Lx
+ * around the y axis through the box centre, 2 the silo r = tanh(y) + 1), with dx =
+ * cbrt(ppc / N_box * Lx Ly Lz) and particle volume dx^3 / ppc.  x: n*3 floats or NULL to only count. */
+PM_API pm_status pm_sample_particles(int device, double Lx, double Ly, double Lz, double radius, double ppc,
+                                     int crop_to_shape, uint32_t attempts, uint32_t passes, uint32_t seed, float* x,
+                                     uint32_t capacity, uint32_t* n, double* dx, double* particle_volume);
+
 /* ---- headless pigment splat --------------------------------------------------------------------
  * BinaryDensityGrid::fillRenderGrid (raytracing/src/raymarch/BinaryDensityGrid.cpp:153-296) without
  * the GL upload: the two-pass anisotropic bilateral splat of the particle latents onto the pigment

@@ -65,6 +65,8 @@ SIGNATURES = {
     "pm_load_checkpoint": [_vp, C.c_char_p],
     "pm_splat_pigments": [_vp, _vp, C.c_int, C.c_float, C.c_float, _vp, _up, _dp, _dp],
     "pm_sample_latent_cylinder": [_vp, C.c_double, C.c_double, C.c_double, _dp, _up],
+    "pm_sample_particles": [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_uint32,
+                            C.c_uint32, C.c_uint32, _fp, C.c_uint32, _up, _dp, _dp],
     "pm_batch_create": [C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(C.c_void_p)],
     "pm_batch_destroy": [_vp],
     "pm_batch_step": [_vp, C.c_uint32],

@@ -1980,3 +1980,58 @@ pm_status pm_splat_pigments(pm_sim* sim, const float* G, int device_ptrs, float 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Poisson-disk particle sampling (sampleParticles, sampling_particles.hpp:12-70)
+// ------------------------------------------------------------------------------------------
+extern "C" {
+
+pm_status pm_sample_particles(int device, double Lx, double Ly, double Lz, double radius, double ppc,
+                              int crop_to_shape, uint32_t attempts, uint32_t passes, uint32_t seed, float* x,
+                              uint32_t capacity, uint32_t* n, double* dx, double* particle_volume) {
+  if (!n) return fail(PM_ERR_INVALID, "NULL count pointer");
+  if (!(radius > 0.0) || !(Lx > 0.0) || !(Ly > 0.0) || !(Lz > 0.0) || !(ppc > 0.0))
+    return fail(PM_ERR_INVALID, "radius, box sides and ppc must be positive");
+  if (crop_to_shape < 0 || crop_to_shape > 2) return fail(PM_ERR_INVALID, "crop_to_shape: 0 box, 1 cylinder, 2 silo");
+  const double cs = radius / std::sqrt(3.0);
+  const long long nx = (long long)std::ceil(Lx / cs), ny = (long long)std::ceil(Ly / cs), nz = (long long)std::ceil(Lz / cs);
+  const long long ncell = nx * ny * nz;
+  if (ncell > (1ll << 31)) return fail(PM_ERR_CAPACITY, "box too large for the sampling grid");
+  CK(cudaSetDevice(device));
+  cudaError_t e = cudaSuccess;
+  if (num_sms() <= 0 && (e = launch_init(device)) != cudaSuccess)
+    return fail(PM_ERR_CUDA, std::string("kernel set-up: ") + cudaGetErrorString(e));
+  float4* d_cells = nullptr;
+  CK(cudaMalloc(&d_cells, sizeof(float4) * (size_t)ncell));
+  e = poisson_fill(d_cells, (int)nx, (int)ny, (int)nz, (float)cs, (float)radius, seed, std::max(passes, 1u),
+                   attempts ? attempts : 30u, 0);
+  std::vector<float4> cells(e == cudaSuccess ? (size_t)ncell : 0);
+  if (e == cudaSuccess) e = cudaMemcpy(cells.data(), d_cells, sizeof(float4) * (size_t)ncell, cudaMemcpyDeviceToHost);
+  cudaFree(d_cells);
+  if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("Poisson sampling: ") + cudaGetErrorString(e));
+  // samples inside the box, in cell order; dx and the particle volume from the uncropped count
+  std::vector<float> pts;
+  size_t square = 0;
+  for (const float4& c : cells) {
+    if (c.w == 0.f || c.x >= Lx || c.y >= Ly || c.z >= Lz) continue;
+    ++square;
+    const double px = c.x - Lx / 2.0, py = c.y, pz = c.z - Lz / 2.0;
+    if (crop_to_shape == 1 && !(px * px + pz * pz < (Lx / 2.0) * (Lx / 2.0))) continue;
+    if (crop_to_shape == 2) {
+      const double rs = std::tanh(py) + 1.0;
+      if (!(px * px + pz * pz < rs * rs)) continue;
+    }
+    pts.insert(pts.end(), {c.x, c.y, c.z});
+  }
+  const double d = std::cbrt(ppc / (double)std::max<size_t>(square, 1) * Lx * Ly * Lz);
+  if (dx) *dx = d;
+  if (particle_volume) *particle_volume = d * d * d / ppc;
+  *n = (uint32_t)(pts.size() / 3);
+  if (x) {
+    if (capacity < *n) return fail(PM_ERR_CAPACITY, "output array holds fewer particles than were sampled");
+    std::memcpy(x, pts.data(), pts.size() * sizeof(float));
+  }
+  return PM_OK;
+}
+
+}  // extern "C"

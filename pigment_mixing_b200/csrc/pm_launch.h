@@ -37,6 +37,10 @@ struct SplatGeom {
 // Two-pass splat into out[dims z][y][x][8] (latent 7 + weight); tmp: same size, pass-1 grid.
 cudaError_t launch_splat(const Params& P, const float* pcur, const uint32_t* meta, const float* G, const SplatGeom& g,
                          float* tmp, float* out, cudaStream_t s);
+// Poisson-disk dart throwing into a background grid of nx*ny*nz cells of side cs (= r / sqrt(3)):
+// cells[c] = (x, y, z, 1) for a cell holding a sample, 0 otherwise.
+cudaError_t poisson_fill(float4* cells, int nx, int ny, int nz, float cs, float r, uint32_t seed, uint32_t passes,
+                         uint32_t attempts, cudaStream_t s);
 // Checkpoint load: grouped host layout of pm_get_particles' unpermute (all F_COUNT fields) -> SoA.
 void launch_load_fields(const Params& P, const float* in, const uint8_t* active, float* pbuf, uint32_t* meta,
                         cudaStream_t s);

@@ -197,6 +197,22 @@ def batch_scenes(n: int = 64, seed: int = 0, min_particles: int = 20000, max_par
     return out
 
 
+def sample_particles(Lx: float, Ly: float, Lz: float, radius: float, ppc: float = 8.0, crop_to_shape: int = 0,
+                     attempts: int = 30, passes: int = 2, seed: int = 42, device: int = 0):
+    """Poisson-disk particles on the GPU (pm_sample_particles, the reference's sampleParticles):
+    returns (x[n, 3] float32, dx, particle_volume)."""
+    import ctypes as C
+    from ._lib import call
+    n = C.c_uint32()
+    dx, vol = C.c_double(), C.c_double()
+    call("pm_sample_particles", device, Lx, Ly, Lz, radius, ppc, crop_to_shape, attempts, passes, seed, None, 0,
+         C.byref(n), C.byref(dx), C.byref(vol))
+    x = np.zeros((n.value, 3), np.float32)
+    call("pm_sample_particles", device, Lx, Ly, Lz, radius, ppc, crop_to_shape, attempts, passes, seed,
+         x.ctypes.data_as(C.POINTER(C.c_float)), n.value, C.byref(n), C.byref(dx), C.byref(vol))
+    return x, dx.value, vol.value
+
+
 def apply(scene: dict, sim) -> None:
     """Load a scene into a Simulation-like object (product Simulation or the oracle wrapper)."""
     if hasattr(sim, "setParticles"):  # product API
