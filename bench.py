@@ -494,7 +494,7 @@ def _batch_leg(args, device, dist, ws):
     sims = make()
     b = Batch(sims)
     t0 = time.perf_counter()
-    tuning, tuned_ms = b.autotune(trial_rounds=3)
+    tuning, tuned_ms = b.autotune(trial_rounds=6)
     tune_s = time.perf_counter() - t0
     b.step(args.warmup)
     stream = torch.cuda.ExternalStream(b.stream(), device=device)

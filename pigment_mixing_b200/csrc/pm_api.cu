@@ -1372,7 +1372,7 @@ pm_status pm_batch::upload_tables() {
     h_sd[s].par_base = par_base[s];
     wp[s] = (double)std::max<uint32_t>(m->np, 1);
     wn[s] = (double)std::max(m->P.node_cap, 1);
-    scan[s + 1] = scan[s] + scan_blocks_for(m->P.node_cap);
+    scan[s + 1] = scan[s] + scan_ctas_for(m->P.node_cap, 16);
     sur = sur || m->P.return_map == 1;
   }
   std::vector<int> unit(n + 1), part, node, p2g, g2p, def, surv;
@@ -1570,9 +1570,10 @@ pm_status pm_batch_create(pm_sim* const* scenes, uint32_t n, pm_batch** out) {
   b->tune.flat_threads = 256;
   b->tune.part_ctas_per_sm = 8;
   b->tune.node_ctas_per_sm = 8;
-  b->tune.p2g_ctas_per_sm = b->occ_p2g;
-  b->tune.g2p_ctas_per_sm = b->occ_g2p;
-  b->tune.def_ctas_per_sm = b->occ_def;
+  // twice the resident CTAs: with static per-scene partitions, finer pieces balance better
+  b->tune.p2g_ctas_per_sm = 2 * b->occ_p2g;
+  b->tune.g2p_ctas_per_sm = 2 * b->occ_g2p;
+  b->tune.def_ctas_per_sm = 2 * b->occ_def;
   b->tune.sur_ctas_per_sm = 8;
   b->tune.chunk_rounds = 64;
   *out = b;

@@ -17,6 +17,7 @@
 //                   position_update.cpp:6-91, simulation.hpp:287-294)
 //   k_epilogue      moveObjects (simulation.cpp:284-291), time += dt, frame bookkeeping
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include <cmath>
 #include "pm_internal.cuh"
@@ -460,22 +461,26 @@ __device__ __forceinline__ void d_scan_local(const Params& P, const Bufs& B, con
   const Ctrl* c = B.ctrl;
   if (c->halt || c->idle) return;
   const int n = c->n_nodes + 1;
-  const int b0 = blk_ * kScanBlock;
-  if (b0 >= n) return;
   __shared__ uint32_t ws[32];
-  uint32_t v[kScanPer];
-  uint32_t tsum = 0;
-  const int i0 = b0 + threadIdx.x * kScanPer;
+  // grid-stride over the 4096-entry scan blocks of this step's box (the launch is sized for a
+  // typical box, not for the grid capacity)
+  for (int sb = blk_; sb * kScanBlock < n; sb += nblk_) {
+    const int b0 = sb * kScanBlock;
+    uint32_t v[kScanPer];
+    uint32_t tsum = 0;
+    const int i0 = b0 + threadIdx.x * kScanPer;
 #pragma unroll
-  for (int k = 0; k < kScanPer; ++k) { v[k] = (i0 + k < n) ? B.cell[i0 + k] : 0u; tsum += v[k]; }
-  uint32_t incl = block_incl_scan(tsum, ws);
-  uint32_t run = incl - tsum;
+    for (int k = 0; k < kScanPer; ++k) { v[k] = (i0 + k < n) ? B.cell[i0 + k] : 0u; tsum += v[k]; }
+    uint32_t incl = block_incl_scan(tsum, ws);
+    uint32_t run = incl - tsum;
 #pragma unroll
-  for (int k = 0; k < kScanPer; ++k) {
-    if (i0 + k < n) B.cell[i0 + k] = run;
-    run += v[k];
+    for (int k = 0; k < kScanPer; ++k) {
+      if (i0 + k < n) B.cell[i0 + k] = run;
+      run += v[k];
+    }
+    if (threadIdx.x == kScanThreads - 1) B.scan_part[sb] = incl;
+    __syncthreads();  // ws is reused by the next block's scan
   }
-  if (threadIdx.x == kScanThreads - 1) B.scan_part[blk_] = incl;
 }
 __global__ void __launch_bounds__(kScanThreads) k_scan_local(Params P, Bufs B) { d_scan_local(P, B, blockIdx.x, gridDim.x); }
 __global__ void __launch_bounds__(kScanThreads) kb_scan_local(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
@@ -520,10 +525,11 @@ __device__ __forceinline__ void d_scan_add(const Params& P, const Bufs& B, const
   const Ctrl* c = B.ctrl;
   if (c->halt || c->idle) return;
   const int n = c->n_nodes + 1;
-  const int b0 = blk_ * kScanBlock;
-  if (b0 >= n || blk_ == 0) return;
-  const uint32_t off = B.scan_part[blk_];
-  for (int i = b0 + threadIdx.x; i < min(b0 + kScanBlock, n); i += kScanThreads) B.cell[i] += off;
+  for (int sb = blk_ > 0 ? blk_ : nblk_; sb * kScanBlock < n; sb += nblk_) {  // block 0 needs no offset
+    const int b0 = sb * kScanBlock;
+    const uint32_t off = B.scan_part[sb];
+    for (int i = b0 + threadIdx.x; i < min(b0 + kScanBlock, n); i += kScanThreads) B.cell[i] += off;
+  }
 }
 __global__ void __launch_bounds__(kScanThreads) k_scan_add(Params P, Bufs B) { d_scan_add(P, B, blockIdx.x, gridDim.x); }
 __global__ void __launch_bounds__(kScanThreads) kb_scan_add(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
@@ -2047,6 +2053,7 @@ __global__ void __launch_bounds__(kThreads) k_stats(Params P, const float* pcur,
 // ------------------------------------------------------------------------------------------
 static int g_num_sms = 0;
 static int g_occ_p2g = 1, g_occ_g2p = 1, g_occ_def = 1;
+int scan_ctas_for(int node_cap, int max_ctas);
 
 cudaError_t launch_init(int device) {
   cudaError_t e = cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -2090,7 +2097,7 @@ const char* kernel_name(int i, const Params& P) {
 void launch_step(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev) {
   const int sms = g_num_sms > 0 ? g_num_sms : 148;
   const int flat_grid = sms * 8;
-  const int scan_blocks = (P.node_cap + 1 + kScanBlock - 1) / kScanBlock;
+  const int scan_blocks = scan_ctas_for(P.node_cap, sms * 2);
   int e = 0;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[e++], s); };
   mark();
@@ -2146,6 +2153,7 @@ void batched_occupancy(int& p2g, int& g2p, int& def) {
   def = def < 1 ? 1 : def;
 }
 int scan_blocks_for(int node_cap) { return (node_cap + 1 + kScanBlock - 1) / kScanBlock; }
+int scan_ctas_for(int node_cap, int max_ctas) { return std::max(1, std::min(scan_blocks_for(node_cap), max_ctas)); }
 
 // One round (one step of every scene that has not reached its target) on stream s.  Each launch
 // covers all scenes: CTAs are statically partitioned across scenes by the offset tables, and each

@@ -69,6 +69,8 @@ int batched_kernels_per_step(bool surrogate);
 const char* batched_kernel_name(int i, bool surrogate);
 void batched_occupancy(int& p2g, int& g2p, int& def);
 int scan_blocks_for(int node_cap);
+// CTAs of the grid-stride scan passes: one per scan block up to max_ctas.
+int scan_ctas_for(int node_cap, int max_ctas);
 void mlp_infer_batched(const SceneDev* sd, const int* off, int ns, int ctas, cudaStream_t s);
 
 }  // namespace pm
