@@ -571,7 +571,7 @@ constexpr int kThreads = 128;  // threads per CTA of the brick kernels
 #endif
 // Unroll factor of the x-layer loop of the 27-node gathers (G2P, deformation update).
 #ifndef PM_GATHER_UNROLL_X
-#define PM_GATHER_UNROLL_X 3
+#define PM_GATHER_UNROLL_X 1
 #endif
 constexpr int kGatherUnrollX = PM_GATHER_UNROLL_X;
 constexpr int kWarps = kThreads / 32;
