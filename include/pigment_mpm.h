@@ -99,6 +99,15 @@ PM_API pm_status pm_set_particles(pm_sim* sim, uint32_t n, const float* x, const
  * delta_gamma); active: n bytes (0/1). */
 PM_API pm_status pm_get_particles(pm_sim* sim, float* x, float* v, float* latent, float* diffusion, uint8_t* active,
                            float* F, float* B, float* plastic);
+/* The per-frame readback of MPMIntegrationSim::recountParticles (MPMIntegrationSim.cpp:100-116)
+ * without waiting for it: the fields are gathered into original order behind the steps issued so
+ * far and copied to the host on a separate stream, so steps issued afterwards overlap the copy.
+ * The host arrays must stay valid (and should be pinned: pageable memory makes the copy
+ * synchronous) until pm_wait_particles returns; any other readback call waits first. */
+PM_API pm_status pm_get_particles_async(pm_sim* sim, float* x, float* v, float* latent, float* diffusion,
+                                        uint8_t* active);
+/* Waits for the last pm_get_particles_async to land in its host arrays. */
+PM_API pm_status pm_wait_particles(pm_sim* sim);
 
 /* ---- object plugins --------------------------------------------------------------------- */
 /* ObjectPlate(pos, type, bc, friction, pos_lower, pos_upper, vx, vy, vz, vmin_factor,

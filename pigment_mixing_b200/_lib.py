@@ -30,6 +30,8 @@ SIGNATURES = {
     "pm_load_sim_config": [_vp, C.c_char_p],
     "pm_set_particles": [_vp, C.c_uint32, _fp, _fp, _fp],
     "pm_get_particles": [_vp, _fp, _fp, _fp, _fp, _u8p, _fp, _fp, _fp],
+    "pm_get_particles_async": [_vp, _fp, _fp, _fp, _fp, _u8p],
+    "pm_wait_particles": [_vp],
     "pm_add_plate": [_vp, C.c_double, C.c_int, C.c_int] + [C.c_double] * 8,
     "pm_add_spatula": [_vp, C.c_int, C.c_double, _fp, C.c_uint32],
     "pm_add_spatula_file": [_vp, C.c_int, C.c_double, C.c_char_p],

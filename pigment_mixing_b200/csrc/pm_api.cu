@@ -143,8 +143,19 @@ struct pm_sim {
   Params P{};
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   bool graphs_dirty = true;
+  // asynchronous particle readback: copies out of d_unperm run on their own stream
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_unperm = nullptr, ev_copied = nullptr;
+  bool copy_pending = false;
 
   ~pm_sim();
+  // Waits for an asynchronous readback still copying out of d_unperm / d_active.
+  pm_status wait_copy() {
+    if (!copy_pending) return PM_OK;
+    copy_pending = false;
+    const cudaError_t e = cudaEventSynchronize(ev_copied);
+    return e == cudaSuccess ? PM_OK : fail(PM_ERR_CUDA, std::string("particle readback: ") + cudaGetErrorString(e));
+  }
   void free_grid();
   void free_particles();
   pm_status alloc_grid(int bricks);
@@ -160,6 +171,10 @@ struct pm_sim {
 };
 
 pm_sim::~pm_sim() {
+  if (copy_pending) cudaEventSynchronize(ev_copied);
+  if (ev_unperm) cudaEventDestroy(ev_unperm);
+  if (ev_copied) cudaEventDestroy(ev_copied);
+  if (copy_stream) cudaStreamDestroy(copy_stream);
   drop_graphs();
   free_particles();
   free_grid();
@@ -644,6 +659,7 @@ pm_status pm_load_sim_config(pm_sim* sim, const char* path) {
 }
 
 pm_status pm_set_particles(pm_sim* sim, uint32_t n, const float* x, const float* latent, const float* v) {
+  if (sim) { pm_status w = sim->wait_copy(); if (w != PM_OK) return w; }
   if (!sim || (n > 0 && !x)) return fail(PM_ERR_INVALID, "NULL argument");
   if (n >= 0x7fffffffu) return fail(PM_ERR_CAPACITY, "too many particles");
   cudaSetDevice(sim->device);
@@ -693,10 +709,14 @@ pm_status pm_get_particles(pm_sim* sim, float* x, float* v, float* latent, float
   const uint32_t n = sim->np;
   if (n == 0) return PM_OK;
   CK(cudaSetDevice(sim->device));
+  pm_status w = sim->wait_copy();
+  if (w != PM_OK) return w;
   Params p = sim->P;
   p.np = (int)n;
   p.np_stride = sim->np_stride;
-  launch_unpermute(p, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], sim->d_unperm, sim->d_active, sim->stream);
+  const uint32_t mask = (x ? kGrpX : 0u) | (v ? kGrpV : 0u) | (latent ? kGrpLat : 0u) | (diffusion ? kGrpDiff : 0u) |
+                        (F ? kGrpF : 0u) | (Bm ? kGrpB : 0u) | (plastic ? kGrpPlastic : 0u);
+  launch_unpermute(p, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], sim->d_unperm, sim->d_active, sim->stream, mask);
   CK(cudaGetLastError());
   auto fetch = [&](int f0, int nf, float* dst) -> pm_status {
     if (!dst) return PM_OK;
@@ -715,6 +735,51 @@ pm_status pm_get_particles(pm_sim* sim, float* x, float* v, float* latent, float
   if (active) CK(cudaMemcpyAsync(active, sim->d_active, n, cudaMemcpyDeviceToHost, sim->stream));
   CK(cudaStreamSynchronize(sim->stream));
   return PM_OK;
+}
+
+pm_status pm_get_particles_async(pm_sim* sim, float* x, float* v, float* latent, float* diffusion, uint8_t* active) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  const uint32_t n = sim->np;
+  if (n == 0) return PM_OK;
+  CK(cudaSetDevice(sim->device));
+  pm_status w = sim->wait_copy();  // the previous readback still owns the staging buffer
+  if (w != PM_OK) return w;
+  if (!sim->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&sim->copy_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&sim->ev_unperm, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&sim->ev_copied, cudaEventDisableTiming));
+  }
+  Params p = sim->P;
+  p.np = (int)n;
+  p.np_stride = sim->np_stride;
+  const uint32_t mask = (x ? kGrpX : 0u) | (v ? kGrpV : 0u) | (latent ? kGrpLat : 0u) | (diffusion ? kGrpDiff : 0u);
+  // the unpermute runs on the step stream (ordered after the steps issued so far); the copies wait
+  // for it on the copy stream, so steps issued next overlap them
+  launch_unpermute(p, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], sim->d_unperm, sim->d_active, sim->stream, mask);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(sim->ev_unperm, sim->stream));
+  CK(cudaStreamWaitEvent(sim->copy_stream, sim->ev_unperm, 0));
+  auto fetch = [&](int f0, int nf, float* dst) -> pm_status {
+    if (!dst) return PM_OK;
+    CK(cudaMemcpyAsync(dst, sim->d_unperm + (size_t)f0 * n, (size_t)n * nf * sizeof(float), cudaMemcpyDeviceToHost,
+                       sim->copy_stream));
+    return PM_OK;
+  };
+  pm_status s;
+  if ((s = fetch(F_X, 3, x)) != PM_OK) return s;
+  if ((s = fetch(F_V, 3, v)) != PM_OK) return s;
+  if ((s = fetch(F_LAT, 7, latent)) != PM_OK) return s;
+  if ((s = fetch(F_DIFF, 1, diffusion)) != PM_OK) return s;
+  if (active) CK(cudaMemcpyAsync(active, sim->d_active, n, cudaMemcpyDeviceToHost, sim->copy_stream));
+  CK(cudaEventRecord(sim->ev_copied, sim->copy_stream));
+  sim->copy_pending = true;
+  return PM_OK;
+}
+
+pm_status pm_wait_particles(pm_sim* sim) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  CK(cudaSetDevice(sim->device));
+  return sim->wait_copy();
 }
 
 pm_status pm_add_plate(pm_sim* sim, double pos, int plate_type, int bc, double friction, double pos_lower,
@@ -1772,7 +1837,9 @@ pm_status pm_save_particle_data(pm_sim* sim, const char* directory, const char* 
   if (!sim || !directory) return fail(PM_ERR_INVALID, "NULL argument");
   if (!sim->prepared) return fail(PM_ERR_STATE, "call pm_prepare first");
   CK(cudaSetDevice(sim->device));
-  pm_status s = sim->sync_ctrl();
+  pm_status s = sim->wait_copy();
+  if (s != PM_OK) return s;
+  s = sim->sync_ctrl();
   if (s != PM_OK) return s;
   const uint32_t n = sim->np;
   Params p = sim->P;
@@ -1835,7 +1902,9 @@ pm_status pm_save_checkpoint(pm_sim* sim, const char* path) {
   if (!sim || !path) return fail(PM_ERR_INVALID, "NULL argument");
   if (!sim->prepared) return fail(PM_ERR_STATE, "call pm_prepare first");
   CK(cudaSetDevice(sim->device));
-  pm_status s = sim->sync_ctrl();
+  pm_status s = sim->wait_copy();
+  if (s != PM_OK) return s;
+  s = sim->sync_ctrl();
   if (s != PM_OK) return s;
   const uint32_t n = sim->np;
   Params p = sim->P;

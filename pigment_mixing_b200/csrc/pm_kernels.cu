@@ -1971,13 +1971,19 @@ __constant__ int c_group_base[F_COUNT] = {0, 0, 0, 3, 3, 3, 6, 6, 6, 6, 6, 6, 6,
                                           24, 24, 24, 24, 24, 24, 24, 31, 32, 32, 32, 32, 36, 36, 36, 36, 36, 36};
 __constant__ int c_group_width[F_COUNT] = {3, 3, 3, 3, 3, 3, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9,
                                            7, 7, 7, 7, 7, 7, 7, 1, 4, 4, 4, 4, 6, 6, 6, 6, 6, 6};
-__global__ void k_unpermute(Params P, const float* pcur, const uint32_t* meta, float* out, uint8_t* active_out) {
+// Field group of each field (x, v, B, F, latent, diffusion, plastic, tau = groups 0..7): k_unpermute
+// copies only the groups whose bit is set in group_mask.
+__constant__ int c_group_id[F_COUNT] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 2, 2, 2, 2, 2, 2, 3, 3, 3, 3, 3, 3, 3, 3, 3,
+                                        4, 4, 4, 4, 4, 4, 4, 5, 6, 6, 6, 6, 7, 7, 7, 7, 7, 7};
+__global__ void k_unpermute(Params P, const float* pcur, const uint32_t* meta, float* out, uint8_t* active_out,
+                            uint32_t group_mask) {
   const int S = P.np_stride, np = P.np;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
     const uint32_t m = meta[i];
     const uint32_t pid = m & ~kInactiveBit;
     if (pid >= (uint32_t)np) continue;
     for (int f = 0; f < F_COUNT; ++f) {
+      if (!((group_mask >> c_group_id[f]) & 1u)) continue;
       const int gb = c_group_base[f], gw = c_group_width[f];
       out[(size_t)gb * np + (size_t)pid * gw + (f - gb)] = pcur[f * S + i];
     }
@@ -2200,9 +2206,9 @@ void launch_reduce_state(const Params& P, const float* pcur, const uint32_t* met
   k_reduce_state<<<sms * 4, kThreads, 0, s>>>(P, pcur, meta, ctrl);
 }
 void launch_unpermute(const Params& P, const float* pcur, const uint32_t* meta, float* out, uint8_t* active,
-                      cudaStream_t s) {
+                      cudaStream_t s, uint32_t group_mask) {
   const int sms = g_num_sms > 0 ? g_num_sms : 148;
-  k_unpermute<<<sms * 4, 256, 0, s>>>(P, pcur, meta, out, active);
+  k_unpermute<<<sms * 4, 256, 0, s>>>(P, pcur, meta, out, active, group_mask);
 }
 // Per particle, in original order: the reference's PLY vertex row (save_data.cpp:7-166) -- x, v,
 // pressure p = -tr(tau)/3, deviatoric stress q = q_prefac |tau + p I|, Je = det F, eps_pl_vol,

@@ -16,8 +16,11 @@ size_t g2p_smem_bytes();
 // One full step on stream s; with ev, events before and after every kernel (kernels_per_step + 1).
 void launch_step(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev = nullptr);
 void launch_reduce_state(const Params& P, const float* pcur, const uint32_t* meta, Ctrl* ctrl, cudaStream_t s);
+// Field groups for launch_unpermute's mask: x, v, B, F, latent, diffusion, plastic, tau.
+enum : uint32_t { kGrpX = 1u, kGrpV = 2u, kGrpB = 4u, kGrpF = 8u, kGrpLat = 16u, kGrpDiff = 32u, kGrpPlastic = 64u,
+                  kGrpTau = 128u, kGrpAll = 255u };
 void launch_unpermute(const Params& P, const float* pcur, const uint32_t* meta, float* out, uint8_t* active,
-                      cudaStream_t s);
+                      cudaStream_t s, uint32_t group_mask = kGrpAll);
 void launch_upload(const Params& P, const float* x, const float* lat, const float* v, float* pbuf, uint32_t* meta,
                    cudaStream_t s);
 void launch_stats(const Params& P, const float* pcur, const uint32_t* meta, double* acc, cudaStream_t s, int cyl = 0,

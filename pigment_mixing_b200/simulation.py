@@ -235,6 +235,14 @@ class Simulation:
         """Copy particle fields into caller-owned float32 arrays (e.g. pinned host buffers)."""
         call("pm_get_particles", self._h, _fp(x), _fp(v), _fp(latent), _fp(diffusion), None, None, None, None)
 
+    def readIntoAsync(self, x=None, latent=None, diffusion=None, v=None) -> None:
+        """Start copying particle fields into caller-owned (pinned) float32 arrays; steps issued
+        afterwards overlap the copy.  Call waitReadback() before using the arrays."""
+        call("pm_get_particles_async", self._h, _fp(x), _fp(v), _fp(latent), _fp(diffusion), None)
+
+    def waitReadback(self) -> None:
+        call("pm_wait_particles", self._h)
+
     @property
     def particles(self) -> Particles:
         return self.getParticles()

@@ -191,3 +191,27 @@ def test_particle_boundaries_deactivate_like_reference():
     assert po["active"].sum() < len(sc["x"])
     assert np.array_equal(pg.active, po["active"])
     assert np.abs(pg.x - po["x"]).max() <= 1e-4
+
+
+def test_async_readback_matches_sync_readback(small_scene):
+    """pm_get_particles_async into pinned buffers, overlapped with further steps, delivers the
+    state of the moment it was issued (the render loop's per-frame readback)."""
+    import torch
+    from pigment_mixing_b200 import Simulation, scenes
+    g = Simulation(0)
+    scenes.apply(small_scene, g)
+    g.prepareSimulation()
+    g.advance(3)
+    ref = g.getParticles(fields=("x", "latent", "diffusion"))
+    n = len(small_scene["x"])
+    ox = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    ol = torch.empty((n, 7), dtype=torch.float32).pin_memory()
+    od = torch.empty((n,), dtype=torch.float32).pin_memory()
+    g.readIntoAsync(x=ox.numpy(), latent=ol.numpy(), diffusion=od.numpy())
+    g.advance(4)  # overlaps the copy; must not change what it delivers
+    g.waitReadback()
+    assert np.array_equal(ox.numpy(), ref.x)
+    assert np.array_equal(ol.numpy(), ref.latent)
+    assert np.array_equal(od.numpy(), ref.diffusion)
+    now = g.getParticles(fields=("x",))  # a sync readback after an async one
+    assert not np.array_equal(now.x, ref.x)
