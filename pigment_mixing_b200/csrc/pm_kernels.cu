@@ -593,18 +593,18 @@ __device__ __forceinline__ int tile_pad(int tn) {  // logical node (x*36 + y*6 +
 // Per-particle data staged by a warp for its node-parallel scatter: the values every lane reads,
 // grouped into float4s (one 128-bit broadcast load each).  The B-spline weights are not staged:
 // each lane evaluates the weight of its own stencil node from the particle's position inside its
-// base cell (see StencilPoly).
-struct __align__(16) StageP2G {
-  float4 f;   // fx fy fz diff            (f = (x - x_base) / dx, in [0.5, 1.5))
-  float4 a;   // q0 q1 q2 lat0            (q = v - D B r)
-  float4 c0;  // C0x C0y C0z C1x          (C = D dx B, columns)
-  float4 c1;  // C1y C1z C2x C2y
-  float4 c2;  // C2z tau_xx tau_yy tau_zz
-  float4 t;   // tau_xy tau_xz tau_yz lat1
-  float4 l0;  // lat2 lat3 lat4 lat5
-  float4 l1;  // lat6 - - -
-};
-static_assert(sizeof(StageP2G) == 32 * 4, "stage size");
+// base cell (see StencilPoly).  The stage is stored field-major ([8 float4][32 particles] per
+// warp): lane i's 128-bit stores of particle i then fall on consecutive banks (a particle-major
+// 128-byte record would put the 8 lanes of each store phase on the same four banks).
+constexpr int kStageP2G = 8;  // float4s per staged particle:
+//   0 f   fx fy fz diff            (f = (x - x_base) / dx, in [0.5, 1.5))
+//   1 a   q0 q1 q2 lat0            (q = v - D B r)
+//   2 c0  C0x C0y C0z C1x          (C = D dx B, columns)
+//   3 c1  C1y C1z C2x C2y
+//   4 c2  C2z tau_xx tau_yy tau_zz
+//   5 t   tau_xy tau_xz tau_yz lat1
+//   6 l0  lat2 lat3 lat4 lat5
+//   7 l1  lat6 - - -
 
 // The quadratic B-spline (tools.hpp:153-177) of stencil node k in {0, 1, 2} as a polynomial of the
 // position f in [0.5, 1.5) inside the base cell: N0 = (1.5 - f)^2 / 2, N1 = 3/4 - (f - 1)^2,
@@ -623,7 +623,7 @@ struct StencilPoly {
   __device__ __forceinline__ float dN(float f) const { return fmaf(d1, f, d0); }
 };
 
-size_t p2g_smem_bytes() { return sizeof(float) * kP2GCh * kTileStride + sizeof(StageP2G) * kThreads; }
+size_t p2g_smem_bytes() { return sizeof(float) * kP2GCh * kTileStride + sizeof(float4) * kStageP2G * kThreads; }
 
 
 __device__ __forceinline__ int tile_to_node(int tn, int bx, int by, int bz, const Ctrl* c) {
@@ -651,10 +651,10 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
   if (c->halt || c->idle) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* tile = reinterpret_cast<float*>(smem_raw);                       // [kP2GCh][216]
-  StageP2G* stw = reinterpret_cast<StageP2G*>(tile + kP2GCh * kTileStride);  // [kWarps][32]
+  float4* stw = reinterpret_cast<float4*>(tile + kP2GCh * kTileStride);  // [kWarps][kStageP2G][32]
   const int S = P.np_stride;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  StageP2G* st = stw + warp * 32;
+  float4* st = stw + warp * kStageP2G * 32;
   const int la = lane / 9, lb = (lane / 3) % 3, lc = lane % 3;
   const float fa = (float)la, fb = (float)lb, fc = (float)lc;
   const float D = P.apicD, dx = P.dx;
@@ -676,7 +676,6 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
       int cl = -1;
       if (lane < n) {
         const uint32_t o = B.sorted[c0 + lane];
-        StageP2G& sp = st[lane];
         AxisW aw[3];
         float r[3];
 #pragma unroll
@@ -701,14 +700,14 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
         for (int k = 0; k < 6; ++k) tau[k] = B.pin[(F_TAU + k) * S + o];
 #pragma unroll
         for (int k = 0; k < 7; ++k) lat[k] = B.pin[(F_LAT + k) * S + o];
-        sp.f = make_float4(r[0] * P.inv_dx, r[1] * P.inv_dx, r[2] * P.inv_dx, B.pin[F_DIFF * S + o]);
-        sp.a = make_float4(q[0], q[1], q[2], lat[0]);
-        sp.c0 = make_float4(C[0], C[1], C[2], C[3]);
-        sp.c1 = make_float4(C[4], C[5], C[6], C[7]);
-        sp.c2 = make_float4(C[8], tau[0], tau[1], tau[2]);
-        sp.t = make_float4(tau[3], tau[4], tau[5], lat[1]);
-        sp.l0 = make_float4(lat[2], lat[3], lat[4], lat[5]);
-        sp.l1 = make_float4(lat[6], 0.f, 0.f, 0.f);
+        st[0 * 32 + lane] = make_float4(r[0] * P.inv_dx, r[1] * P.inv_dx, r[2] * P.inv_dx, B.pin[F_DIFF * S + o]);
+        st[1 * 32 + lane] = make_float4(q[0], q[1], q[2], lat[0]);
+        st[2 * 32 + lane] = make_float4(C[0], C[1], C[2], C[3]);
+        st[3 * 32 + lane] = make_float4(C[4], C[5], C[6], C[7]);
+        st[4 * 32 + lane] = make_float4(C[8], tau[0], tau[1], tau[2]);
+        st[5 * 32 + lane] = make_float4(tau[3], tau[4], tau[5], lat[1]);
+        st[6 * 32 + lane] = make_float4(lat[2], lat[3], lat[4], lat[5]);
+        st[7 * 32 + lane] = make_float4(lat[6], 0.f, 0.f, 0.f);
       }
       // runs of equal cells among the warp's particles
       const int prev = __shfl_up_sync(0xffffffffu, cl, 1);
@@ -724,8 +723,8 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
 #pragma unroll
           for (int k = 0; k < kP2GCh; ++k) acc[k] = 0.f;
           for (int q = s0; q < s1; ++q) {
-            const StageP2G& sp = st[q];
-            const float4 Fr = sp.f, A = sp.a, C0 = sp.c0, C1 = sp.c1, C2 = sp.c2, T = sp.t, L0 = sp.l0, L1 = sp.l1;
+            const float4 Fr = st[0 * 32 + q], A = st[1 * 32 + q], C0 = st[2 * 32 + q], C1 = st[3 * 32 + q];
+            const float4 C2 = st[4 * 32 + q], T = st[5 * 32 + q], L0 = st[6 * 32 + q], L1 = st[7 * 32 + q];
             const float nx = px.N(Fr.x), ny = py.N(Fr.y), nz = pz.N(Fr.z);
             const float nyz = ny * nz;
             const float w = nx * nyz;
@@ -1018,16 +1017,19 @@ __global__ void kb_grid_update(const SceneDev* __restrict__ sd, const int* __res
 // ------------------------------------------------------------------------------------------
 // G2P + mixing + MUSL (velocity update and re-scatter)
 // ------------------------------------------------------------------------------------------
-struct __align__(16) StageMUSL {
-  float4 q;    // q0 q1 q2 fx  (q = v_new - D B_new r; f = position in the base cell, StencilPoly)
-  float4 c0;   // C0x C0y C0z C1x
-  float4 c1;   // C1y C1z C2x C2y
-  float4 c2;   // C2z fy fz -
-};
-static_assert(sizeof(StageMUSL) == 16 * 4, "stage size");
+// The G2P node tile is field-major too: record part k (0..3) of tile node tn at
+// tile[k * kG2PTileStride + tn].  The stride 218 = 2 mod 8 puts the four parts of a node on
+// different bank groups, so the loads of a brick's tile are conflict-free.
+constexpr int kG2PTileStride = 218;
+// MUSL stage, field-major like the P2G stage ([4 float4][32 particles] per warp):
+constexpr int kStageMUSL = 4;  // float4s per staged particle:
+//   0 q   q0 q1 q2 fx  (q = v_new - D B_new r; f = position in the base cell, StencilPoly)
+//   1 c0  C0x C0y C0z C1x
+//   2 c1  C1y C1z C2x C2y
+//   3 c2  C2z fy fz -
 
 size_t g2p_smem_bytes() {
-  return sizeof(float4) * 4 * kTileNodes + sizeof(float) * 4 * kTileStride + sizeof(StageMUSL) * kThreads;
+  return sizeof(float4) * 4 * kG2PTileStride + sizeof(float) * 4 * kTileStride + sizeof(float4) * kStageMUSL * kThreads;
 }
 
 __device__ __forceinline__ float smooth_step(float e0, float e1, float x) {  // g2p.cpp:7-10
@@ -1047,12 +1049,12 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
   const Ctrl* c = B.ctrl;
   if (c->halt || c->idle) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float4* tile = reinterpret_cast<float4*>(smem_raw);              // [216][4]
-  float* mtile = reinterpret_cast<float*>(tile + 4 * kTileNodes);  // [4][kTileStride], padded layout
-  StageMUSL* stw = reinterpret_cast<StageMUSL*>(mtile + 4 * kTileStride);
+  float4* tile = reinterpret_cast<float4*>(smem_raw);                  // [4][kG2PTileStride]
+  float* mtile = reinterpret_cast<float*>(tile + 4 * kG2PTileStride);  // [4][kTileStride], padded layout
+  float4* stw = reinterpret_cast<float4*>(mtile + 4 * kTileStride);  // [kWarps][kStageMUSL][32]
   const int S = P.np_stride;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  StageMUSL* st = stw + warp * 32;
+  float4* st = stw + warp * kStageMUSL * 32;
   const int la = lane / 9, lb = (lane / 3) % 3, lc = lane % 3;
   const float fa = (float)la, fb = (float)lb, fcc = (float)lc;
   const StencilPoly px(la, P.inv_dx), py(lb, P.inv_dx), pz(lc, P.inv_dx);
@@ -1079,7 +1081,8 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
     brick_coords(b, c, bx, by, bz);
     for (int i = threadIdx.x; i < kTileNodes * 4; i += kThreads) {
       const int node = tile_to_node(i >> 2, bx, by, bz, c);
-      tile[i] = node >= 0 ? B.grid[(size_t)node * 4 + (i & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
+      tile[(i & 3) * kG2PTileStride + (i >> 2)] =
+          node >= 0 ? B.grid[(size_t)node * 4 + (i & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
     {
       float4* m4 = reinterpret_cast<float4*>(mtile);
@@ -1119,7 +1122,8 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
               const int tn = ((lx + a) * kTile + (ly + bb)) * kTile + (lz + cz);
               const float w = nxy * aw[2].N[cz];
               const float g0 = dnxy * aw[2].N[cz], g1 = ndxy * aw[2].N[cz], g2 = nxy * aw[2].dN[cz];
-              const float4 R0 = tile[4 * tn], R1 = tile[4 * tn + 1], R2 = tile[4 * tn + 2], R3 = tile[4 * tn + 3];
+              const float4 R0 = tile[tn], R1 = tile[kG2PTileStride + tn], R2 = tile[2 * kG2PTileStride + tn],
+                           R3 = tile[3 * kG2PTileStride + tn];
               const float gv[3] = {R0.x, R0.y, R0.z};
 #pragma unroll
               for (int r = 0; r < 3; ++r) {
@@ -1184,7 +1188,6 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
         for (int k = 0; k < 7; ++k) po[(F_LAT + k) * S + i] = lat[k];
         po[F_DIFF * S + i] = diff;
         if (musl) {
-          StageMUSL& sp = st[lane];
           const float r3[3] = {aw[0].r, aw[1].r, aw[2].r};
           float q[3], C[9];
 #pragma unroll
@@ -1194,10 +1197,10 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
           for (int k = 0; k < 3; ++k)
 #pragma unroll
             for (int qq = 0; qq < 3; ++qq) C[3 * k + qq] = D * dx * Bp[3 * qq + k];
-          sp.q = make_float4(q[0], q[1], q[2], r3[0] * P.inv_dx);
-          sp.c0 = make_float4(C[0], C[1], C[2], C[3]);
-          sp.c1 = make_float4(C[4], C[5], C[6], C[7]);
-          sp.c2 = make_float4(C[8], r3[1] * P.inv_dx, r3[2] * P.inv_dx, 0.f);
+          st[0 * 32 + lane] = make_float4(q[0], q[1], q[2], r3[0] * P.inv_dx);
+          st[1 * 32 + lane] = make_float4(C[0], C[1], C[2], C[3]);
+          st[2 * 32 + lane] = make_float4(C[4], C[5], C[6], C[7]);
+          st[3 * 32 + lane] = make_float4(C[8], r3[1] * P.inv_dx, r3[2] * P.inv_dx, 0.f);
         }
       }
       if (musl) {
@@ -1212,8 +1215,7 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
           if (lane < 27) {
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
             for (int q = s0; q < s1; ++q) {
-              const StageMUSL& sp = st[q];
-              const float4 Q = sp.q, C0 = sp.c0, C1 = sp.c1, C2 = sp.c2;
+              const float4 Q = st[0 * 32 + q], C0 = st[1 * 32 + q], C1 = st[2 * 32 + q], C2 = st[3 * 32 + q];
               const float w = px.N(Q.w) * (py.N(C2.y) * pz.N(C2.z));
               const float wm = w > 1e-25f ? w : 0.f;  // musl.cpp:188
               acc[0] += wm * (Q.x + fa * C0.x + fb * C0.w + fcc * C1.z);

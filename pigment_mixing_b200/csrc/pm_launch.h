@@ -36,6 +36,7 @@ struct SplatGeom {
   int dims[3];
   int ext;
   float sig_s2, sig_c2, inv_h;
+  uint32_t order_stride;  // particle visiting order i -> i * stride mod np (1: sorted order)
 };
 // Two-pass splat into out[dims z][y][x][8] (latent 7 + weight); tmp: same size, pass-1 grid.
 cudaError_t launch_splat(const Params& P, const float* pcur, const uint32_t* meta, const float* G, const SplatGeom& g,

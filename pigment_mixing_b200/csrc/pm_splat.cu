@@ -11,6 +11,7 @@
 //
 // Layout: one warp per particle, lane per voxel of the particle's (2 ext + 1)^3 search box, so the
 // 32 atomics of a warp instruction hit 32 different voxels; two red.global.add.v4.f32 per voxel.
+// Warps visit the cell-sorted particles in the order i -> i * SplatGeom::order_stride mod np.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -34,7 +35,8 @@ __global__ void k_splat(Params P, const float* pcur, const uint32_t* meta, const
   const int warps = gridDim.x * (blockDim.x >> 5);
   const int side = 2 * g.ext + 1, box = side * side * side;
   const float inv_s2 = 1.f / g.sig_s2, inv_c2 = 1.f / g.sig_c2, cut = 9.f * g.sig_s2;
-  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < np; i += warps) {
+  for (int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < np; t += warps) {
+    const int i = (int)(((uint64_t)t * g.order_stride) % (uint32_t)np);
     const uint32_t pid = meta[i] & ~kInactiveBit;
     float x[3], lat[7], Gm[9];
 #pragma unroll
