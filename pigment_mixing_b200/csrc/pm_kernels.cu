@@ -574,6 +574,15 @@ constexpr int kThreads = 128;  // threads per CTA of the brick kernels
 #define PM_GATHER_UNROLL_X 1
 #endif
 constexpr int kGatherUnrollX = PM_GATHER_UNROLL_X;
+// Unroll factor of the per-run particle loops of the node-parallel scatters (P2G, MUSL) and the
+// P2G launch bound (minimum resident CTAs per SM; 0 leaves the register count to the compiler).
+#ifndef PM_SCATTER_UNROLL
+#define PM_SCATTER_UNROLL 1
+#endif
+#ifndef PM_P2G_MINB
+#define PM_P2G_MINB 0
+#endif
+constexpr int kScatterUnroll = PM_SCATTER_UNROLL;
 constexpr int kWarps = kThreads / 32;
 constexpr int kP2GCh = 15;
 
@@ -722,6 +731,7 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
           float acc[kP2GCh];
 #pragma unroll
           for (int k = 0; k < kP2GCh; ++k) acc[k] = 0.f;
+#pragma unroll kScatterUnroll
           for (int q = s0; q < s1; ++q) {
             const float4 Fr = st[0 * 32 + q], A = st[1 * 32 + q], C0 = st[2 * 32 + q], C1 = st[3 * 32 + q];
             const float4 C2 = st[4 * 32 + q], T = st[5 * 32 + q], L0 = st[6 * 32 + q], L1 = st[7 * 32 + q];
@@ -770,7 +780,11 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
     __syncthreads();
   }
 }
+#if PM_P2G_MINB > 0
+__global__ void __launch_bounds__(kThreads, PM_P2G_MINB) k_p2g(Params P, Bufs B) { d_p2g(P, B, blockIdx.x, gridDim.x); }
+#else
 __global__ void __launch_bounds__(kThreads) k_p2g(Params P, Bufs B) { d_p2g(P, B, blockIdx.x, gridDim.x); }
+#endif
 __global__ void __launch_bounds__(kThreads) kb_p2g(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
   int s_, blk_, nblk_;
   batch_slot(off, ns, s_, blk_, nblk_);
@@ -1101,24 +1115,26 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
         for (int d = 0; d < 3; ++d) aw[d] = axis_weights(B.pin[(F_X + d) * S + o], P.anchor[d], dx, P.inv_dx);
         cl = local_cell(aw, c, bx, by, bz);
         const int lx = cl >> 4, ly = (cl >> 2) & 3, lz = cl & 3;
-        float vp[3] = {0.f, 0.f, 0.f}, fp[3] = {0.f, 0.f, 0.f}, Bp[9], L[9], gl[7], gs = 0.f;
+        // Ls: the velocity gradient's symmetric part, accumulated directly (xx, yy, zz and the
+        // doubled off-diagonals xy, xz, yz): only |0.5 (L + L^T)|_F is used
+        float vp[3] = {0.f, 0.f, 0.f}, fp[3] = {0.f, 0.f, 0.f}, Bp[9], Ls[6], gl[7], gs = 0.f;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) { Bp[k] = 0.f; L[k] = 0.f; }
+        for (int k = 0; k < 9; ++k) Bp[k] = 0.f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) Ls[k] = 0.f;
 #pragma unroll
         for (int k = 0; k < 7; ++k) gl[k] = 0.f;
 #pragma unroll kGatherUnrollX
         for (int a = 0; a < 3; ++a) {
-          const float dxa = (float)a * dx - aw[0].r;
+          const float oa = (float)a;
           const float Na = a == 0 ? aw[0].N[0] : (a == 1 ? aw[0].N[1] : aw[0].N[2]);
           const float dNa = a == 0 ? aw[0].dN[0] : (a == 1 ? aw[0].dN[1] : aw[0].dN[2]);
 #pragma unroll
           for (int bb = 0; bb < 3; ++bb) {
-            const float dyb = (float)bb * dx - aw[1].r;
             const float nxy = Na * aw[1].N[bb];
             const float dnxy = dNa * aw[1].N[bb], ndxy = Na * aw[1].dN[bb];
 #pragma unroll
             for (int cz = 0; cz < 3; ++cz) {
-              const float dzc = (float)cz * dx - aw[2].r;
               const int tn = ((lx + a) * kTile + (ly + bb)) * kTile + (lz + cz);
               const float w = nxy * aw[2].N[cz];
               const float g0 = dnxy * aw[2].N[cz], g1 = ndxy * aw[2].N[cz], g2 = nxy * aw[2].dN[cz];
@@ -1129,13 +1145,16 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
               for (int r = 0; r < 3; ++r) {
                 const float wv = gv[r] * w;
                 vp[r] += wv;
-                Bp[3 * r + 0] += wv * dxa;
-                Bp[3 * r + 1] += wv * dyb;
-                Bp[3 * r + 2] += wv * dzc;
-                L[3 * r + 0] += gv[r] * g0;
-                L[3 * r + 1] += gv[r] * g1;
-                L[3 * r + 2] += gv[r] * g2;
+                Bp[3 * r + 0] += wv * oa;
+                if (bb) Bp[3 * r + 1] += wv * (float)bb;
+                if (cz) Bp[3 * r + 2] += wv * (float)cz;
               }
+              Ls[0] += gv[0] * g0;
+              Ls[1] += gv[1] * g1;
+              Ls[2] += gv[2] * g2;
+              Ls[3] += gv[0] * g1 + gv[1] * g0;
+              Ls[4] += gv[0] * g2 + gv[2] * g0;
+              Ls[5] += gv[1] * g2 + gv[2] * g1;
               if (use_flip) { fp[0] += R0.w * w; fp[1] += R1.x * w; fp[2] += R1.y * w; }
               gl[0] += R1.z * w; gl[1] += R1.w * w;
               gl[2] += R2.x * w; gl[3] += R2.y * w; gl[4] += R2.z * w; gl[5] += R2.w * w;
@@ -1144,6 +1163,12 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
             }
           }
         }
+        // B = sum w v (x_i - x_p)^T, accumulated above with the node offsets o in {0, 1, 2}
+        // (x_i - x_p = o dx - r): B = dx sum w v o^T - (sum w v) r^T
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int k = 0; k < 3; ++k) Bp[3 * r + k] = dx * Bp[3 * r + k] - vp[r] * aw[k].r;
         if (!apic) for (int k = 0; k < 9; ++k) Bp[k] = 0.f;
         // particle state read after the gather (not live across it)
 #pragma unroll
@@ -1154,11 +1179,8 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
           for (int d = 0; d < 3; ++d) vold[d] = B.pin[(F_V + d) * S + o];
         }
         // diffusion factor |0.5 (L + L^T)|_F (g2p.cpp:98-101)
-        float s2 = 0.f;
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-          for (int q = 0; q < 3; ++q) { float sv = 0.5f * (L[3 * r + q] + L[3 * q + r]); s2 += sv * sv; }
+        const float s2 = Ls[0] * Ls[0] + Ls[1] * Ls[1] + Ls[2] * Ls[2] +
+                         0.5f * (Ls[3] * Ls[3] + Ls[4] * Ls[4] + Ls[5] * Ls[5]);
         const float diff = sqrtf(s2);
         // mixing (g2p.cpp:105-130)
         const float mixf = smooth_step(P.D_edge0, P.D_edge1, gs);
@@ -1214,6 +1236,7 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
           const int cell = __shfl_sync(0xffffffffu, cl, s0);
           if (lane < 27) {
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll kScatterUnroll
             for (int q = s0; q < s1; ++q) {
               const float4 Q = st[0 * 32 + q], C0 = st[1 * 32 + q], C1 = st[2 * 32 + q], C2 = st[3 * 32 + q];
               const float w = px.N(Q.w) * (py.N(C2.y) * pz.N(C2.z));
