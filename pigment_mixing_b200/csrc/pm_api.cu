@@ -1201,17 +1201,17 @@ pm_status pm_get_grid(pm_sim* sim, double origin[3], uint32_t dims[3], float* ma
         const size_t l = ((size_t)i * c->dims[1] + j) * c->dims[2] + k;
         const size_t b = ((size_t)(i >> 2) * c->nb[1] + (j >> 2)) * c->nb[2] + (k >> 2);
         const size_t n = b * kBrickNodes + (i & 3) * 16 + (j & 3) * 4 + (k & 3);
-        // updated record: [v xyz, flip x | flip yz, lat0, lat1 | lat2..lat5 | lat6, shear, mass, -]
+        // updated record: [v xyz, lat0 | lat1..lat4 | lat5, lat6, shear, mass | flip xyz, -]
         const float4 r0 = g[n * 4], r1 = g[n * 4 + 1], r2 = g[n * 4 + 2], r3 = g[n * 4 + 3];
-        const bool has = r3.z > 0.f;
-        if (mass) mass[l] = has ? r3.z : 0.f;
+        const bool has = r2.w > 0.f;
+        if (mass) mass[l] = has ? r2.w : 0.f;
         if (v_update) { v_update[3 * l] = has ? r0.x : 0.f; v_update[3 * l + 1] = has ? r0.y : 0.f; v_update[3 * l + 2] = has ? r0.z : 0.f; }
-        if (flip) { flip[3 * l] = has ? r0.w : 0.f; flip[3 * l + 1] = has ? r1.x : 0.f; flip[3 * l + 2] = has ? r1.y : 0.f; }
+        if (flip) { flip[3 * l] = has ? r3.x : 0.f; flip[3 * l + 1] = has ? r3.y : 0.f; flip[3 * l + 2] = has ? r3.z : 0.f; }
         if (latent) {
-          const float lv[7] = {r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.x};
+          const float lv[7] = {r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y};
           for (int q = 0; q < 7; ++q) latent[7 * l + q] = has ? lv[q] : 0.f;
         }
-        if (shear) shear[l] = has ? r3.y : 0.f;
+        if (shear) shear[l] = has ? r2.z : 0.f;
         if (v_musl) {
           const float4 mm = m[n];
           const float inv = mm.w > 0.f ? 1.f / mm.w : 0.f;

@@ -1011,11 +1011,12 @@ __device__ __forceinline__ void d_grid_update(const Params& P, const Bufs& B, co
     const int gi[3] = {c->g0[0] + bx * 4 + (loc >> 4), c->g0[1] + by * 4 + ((loc >> 2) & 3), c->g0[2] + bz * 4 + (loc & 3)};
     float X[3] = {node_pos(gi[0], P.anchor[0], P.dx), node_pos(gi[1], P.anchor[1], P.dx), node_pos(gi[2], P.anchor[2], P.dx)};
     boundary_collision(c, dtf, P.dx, X, nv, err);
-    // updated record, laid out as the G2P tile reads it (4 x 16 B per node)
-    rec[0] = make_float4(nv[0], nv[1], nv[2], nv[0] - v[0]);
-    rec[1] = make_float4(nv[1] - v[1], nv[2] - v[2], lat[0], lat[1]);
-    rec[2] = make_float4(lat[2], lat[3], lat[4], lat[5]);
-    rec[3] = make_float4(lat[6], shear, mi, 0.f);
+    // updated record, laid out as the G2P tile reads it (4 x 16 B per node): the pure-APIC G2P
+    // reads the first three, the FLIP velocity change sits in the fourth
+    rec[0] = make_float4(nv[0], nv[1], nv[2], lat[0]);
+    rec[1] = make_float4(lat[1], lat[2], lat[3], lat[4]);
+    rec[2] = make_float4(lat[5], lat[6], shear, mi);
+    rec[3] = make_float4(nv[0] - v[0], nv[1] - v[1], nv[2] - v[2], 0.f);
   }
   if (err) atomicOr(&B.ctrl->error_flags, err);
 }
@@ -1094,6 +1095,7 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
     int bx, by, bz;
     brick_coords(b, c, bx, by, bz);
     for (int i = threadIdx.x; i < kTileNodes * 4; i += kThreads) {
+      if (!kFlip && (i & 3) == 3) continue;  // the velocity change is read by FLIP only
       const int node = tile_to_node(i >> 2, bx, by, bz, c);
       tile[(i & 3) * kG2PTileStride + (i >> 2)] =
           node >= 0 ? B.grid[(size_t)node * 4 + (i & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1126,7 +1128,7 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
         for (int k = 0; k < 7; ++k) gl[k] = 0.f;
 #pragma unroll kGatherUnrollX
         for (int a = 0; a < 3; ++a) {
-          const float oa = (float)a;
+          const float oa = (float)(a - 1);
           const float Na = a == 0 ? aw[0].N[0] : (a == 1 ? aw[0].N[1] : aw[0].N[2]);
           const float dNa = a == 0 ? aw[0].dN[0] : (a == 1 ? aw[0].dN[1] : aw[0].dN[2]);
 #pragma unroll
@@ -1138,16 +1140,15 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
               const int tn = ((lx + a) * kTile + (ly + bb)) * kTile + (lz + cz);
               const float w = nxy * aw[2].N[cz];
               const float g0 = dnxy * aw[2].N[cz], g1 = ndxy * aw[2].N[cz], g2 = nxy * aw[2].dN[cz];
-              const float4 R0 = tile[tn], R1 = tile[kG2PTileStride + tn], R2 = tile[2 * kG2PTileStride + tn],
-                           R3 = tile[3 * kG2PTileStride + tn];
+              const float4 R0 = tile[tn], R1 = tile[kG2PTileStride + tn], R2 = tile[2 * kG2PTileStride + tn];
               const float gv[3] = {R0.x, R0.y, R0.z};
 #pragma unroll
               for (int r = 0; r < 3; ++r) {
                 const float wv = gv[r] * w;
                 vp[r] += wv;
                 Bp[3 * r + 0] += wv * oa;
-                if (bb) Bp[3 * r + 1] += wv * (float)bb;
-                if (cz) Bp[3 * r + 2] += wv * (float)cz;
+                if (bb != 1) Bp[3 * r + 1] += bb == 0 ? -wv : wv;
+                if (cz != 1) Bp[3 * r + 2] += cz == 0 ? -wv : wv;
               }
               Ls[0] += gv[0] * g0;
               Ls[1] += gv[1] * g1;
@@ -1155,20 +1156,25 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
               Ls[3] += gv[0] * g1 + gv[1] * g0;
               Ls[4] += gv[0] * g2 + gv[2] * g0;
               Ls[5] += gv[1] * g2 + gv[2] * g1;
-              if (use_flip) { fp[0] += R0.w * w; fp[1] += R1.x * w; fp[2] += R1.y * w; }
-              gl[0] += R1.z * w; gl[1] += R1.w * w;
-              gl[2] += R2.x * w; gl[3] += R2.y * w; gl[4] += R2.z * w; gl[5] += R2.w * w;
-              gl[6] += R3.x * w;
-              gs += R3.y * w;
+              if (use_flip) {
+                const float4 R3 = tile[3 * kG2PTileStride + tn];
+                fp[0] += R3.x * w; fp[1] += R3.y * w; fp[2] += R3.z * w;
+              }
+              gl[0] += R0.w * w;
+              gl[1] += R1.x * w; gl[2] += R1.y * w; gl[3] += R1.z * w; gl[4] += R1.w * w;
+              gl[5] += R2.x * w; gl[6] += R2.y * w;
+              gs += R2.z * w;
             }
           }
         }
-        // B = sum w v (x_i - x_p)^T, accumulated above with the node offsets o in {0, 1, 2}
-        // (x_i - x_p = o dx - r): B = dx sum w v o^T - (sum w v) r^T
+        // B = sum w v (x_i - x_p)^T, accumulated above with the node offsets o in {-1, 0, 1} from
+        // the stencil's middle node (x_i - x_p = o dx - (r - dx)): B = dx sum w v o^T - (sum w v)
+        // (r - dx)^T.  Centring keeps both terms within half a cell (r - dx is exact), so their
+        // difference loses no more than the direct sum would.
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
-          for (int k = 0; k < 3; ++k) Bp[3 * r + k] = dx * Bp[3 * r + k] - vp[r] * aw[k].r;
+          for (int k = 0; k < 3; ++k) Bp[3 * r + k] = dx * Bp[3 * r + k] - vp[r] * (aw[k].r - dx);
         if (!apic) for (int k = 0; k < 9; ++k) Bp[k] = 0.f;
         // particle state read after the gather (not live across it)
 #pragma unroll
