@@ -267,6 +267,33 @@ PM_API pm_status pm_splat_pigments(pm_sim* sim, const float* G, int device_ptrs,
                                    float sigma_color, float* voxels, uint32_t dims[3], double origin[3],
                                    double* voxel_size);
 
+/* ---- renderer preprocessing: binary density grid and anisotropy ---------------------------------
+ * BinaryDensityGrid::fillCells / generateNc / fillBDG (raytracing/src/raymarch/BinaryDensityGrid.cpp:
+ * 22-151) on the density voxels of AABBc::fixedAABB (side h = 2 dx over the grid boundaries):
+ * particle counts per voxel, the separable neighbour filter with weights a (voxel) and b (each
+ * neighbour; the reference's state.params 0.75, 0.74), occupancy M = (nc 315/(64 pi h^3) >= iso)
+ * (reference iso 9285; test_all_filled sets every voxel), and M2 / M4, the OR of M over 2^3 and
+ * 4^3 blocks.  Voxel v = x + X (y + Y z); M2 and M4 have ceil(X/2) x ceil(Y/2) x ceil(Z/2) and
+ * ceil(X/4) x ... entries.  cell_count / cell_offset (per voxel) and ids (particle indices of the
+ * binned particles, grouped by voxel; order inside a voxel unspecified) are the binning itself;
+ * each output may be NULL.  M == NULL only fills dims, origin and voxel_size.  occupancy[2]
+ * receives the counts of empty and occupied voxels (state.count).  device_ptrs: the arrays are
+ * device pointers. */
+PM_API pm_status pm_density_grid(pm_sim* sim, float a, float b, float iso, int test_all_filled, int device_ptrs,
+                                 uint32_t* M, uint32_t* M2, uint32_t* M4, uint32_t* cell_count,
+                                 uint32_t* cell_offset, uint32_t* ids, uint32_t dims[3], double origin[3],
+                                 double* voxel_size, uint32_t occupancy[2]);
+/* Classification::countMatrix / countCurrDens (raytracing/src/raymarch/Classification.cpp:38-130):
+ * per particle (original order) the anisotropy matrix G (3x3, row-major, symmetric), its inverse,
+ * |det G| and the anisotropic density, from the neighbours within h found through the binning.
+ * Parameters are the reference's state.s (1400), state.k (4), state.aniso_threshold (15),
+ * state.autoScaleS (1) and state.isAni (1); iso (9285) counts the aggregate particles
+ * (density > iso) into n_aggregate.  Outputs may be NULL.  device_ptrs: the arrays are device
+ * pointers; G from here feeds pm_splat_pigments. */
+PM_API pm_status pm_anisotropy(pm_sim* sim, float s, float k, int threshold, int auto_scale, int is_ani, float iso,
+                               int device_ptrs, float* G, float* G_inv, float* det, float* density,
+                               uint32_t* n_aggregate);
+
 /* ---- batched scenes --------------------------------------------------------------------------
  * No counterpart in the reference, which runs one Simulation per process
  * (R/src/mpm/MPMIntegrationSim.cpp:16-38 creates one).  A batch steps many independent, prepared

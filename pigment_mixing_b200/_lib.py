@@ -66,6 +66,10 @@ SIGNATURES = {
     "pm_save_checkpoint": [_vp, C.c_char_p],
     "pm_load_checkpoint": [_vp, C.c_char_p],
     "pm_splat_pigments": [_vp, _vp, C.c_int, C.c_float, C.c_float, _vp, _up, _dp, _dp],
+    "pm_density_grid": [_vp, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _up,
+                        _dp, _dp, _up],
+    "pm_anisotropy": [_vp, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _vp, _vp, _vp, _vp,
+                      _up],
     "pm_sample_latent_cylinder": [_vp, C.c_double, C.c_double, C.c_double, _dp, _up],
     "pm_sample_particles": [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_uint32,
                             C.c_uint32, C.c_uint32, _fp, C.c_uint32, _up, _dp, _dp],

@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libpigment_mpm.so")
-SOURCES = ["pm_kernels.cu", "pm_api.cu", "pm_mlp.cu", "pm_noalloc.cu", "pm_splat.cu", "pm_sampling.cu"]
+SOURCES = ["pm_kernels.cu", "pm_api.cu", "pm_mlp.cu", "pm_noalloc.cu", "pm_splat.cu", "pm_sampling.cu", "pm_render.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",

@@ -152,6 +152,9 @@ struct pm_sim {
   // between calls so that a renderer splatting every frame allocates once
   float* d_splat = nullptr;
   size_t splat_bytes = 0;
+  // scratch of the density-grid and anisotropy passes, grown on demand
+  void* d_render = nullptr;
+  size_t render_bytes = 0;
 
   ~pm_sim();
   // Waits for an asynchronous readback still copying out of d_unperm / d_active.
@@ -190,6 +193,7 @@ pm_sim::~pm_sim() {
   if (d_mlp) cudaFree(d_mlp);
   if (d_slog) cudaFree(d_slog);
   if (d_splat) cudaFree(d_splat);
+  if (d_render) cudaFree(d_render);
   free_surrogate_queue();
   if (stream) cudaStreamDestroy(stream);
 }
@@ -2075,6 +2079,173 @@ pm_status pm_splat_pigments(pm_sim* sim, const float* G, int device_ptrs, float 
   if (e == cudaSuccess) e = cudaStreamSynchronize(sim->stream);
   release();
   if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("pigment splat: ") + cudaGetErrorString(e));
+  return PM_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// renderer preprocessing: binary density grid (BinaryDensityGrid::fillBDG) and anisotropy
+// (Classification::countDensities)
+// ------------------------------------------------------------------------------------------
+namespace {
+
+// AABBc::fixedAABB (AABBc.cpp:10-25) over the simulation's grid boundaries, in float as there
+DensityGeom density_geom(const pm_sim* sim) {
+  DensityGeom g{};
+  const float h = (float)(2.0 * sim->hp.dx);
+  g.h = h;
+  for (int d = 0; d < 3; ++d) {
+    const float mn = (float)sim->h_ctrl->low[d], mx = (float)sim->h_ctrl->high[d];
+    g.start[d] = std::floor(mn / h) * h;
+    g.dims[d] = (int)std::ceil((mx - mn) / h) + 1;
+  }
+  return g;
+}
+
+// Grows the render scratch to at least `bytes` and carves the binning / anisotropy arrays.
+pm_status render_scratch(pm_sim* sim, uint32_t ncell, bool aniso, size_t extra, RenderScratch& r, char*& tail) {
+  const size_t core = render_scratch_bytes(sim->np, ncell, aniso);
+  const size_t want = core + (extra + 255) / 256 * 256;
+  if (sim->render_bytes < want) {
+    if (sim->d_render) cudaFree(sim->d_render);
+    sim->d_render = nullptr;
+    sim->render_bytes = 0;
+    if (cudaMalloc(&sim->d_render, want) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(PM_ERR_CUDA, "allocation of the density-grid scratch failed");
+    }
+    sim->render_bytes = want;
+  }
+  const size_t nb = (ncell + 4095) / 4096;
+  uint32_t* u = static_cast<uint32_t*>(sim->d_render);
+  r.counts = u; u += ncell;
+  r.offsets = u; u += ncell;
+  r.bsum = u; u += nb;
+  r.misc = u; u += 4;
+  r.cellid = u; u += sim->np;
+  r.rank = u; u += sim->np;
+  r.ids = u; u += sim->np;
+  float* f = reinterpret_cast<float*>(u);
+  r.Gs = aniso ? f : nullptr;
+  r.dets = aniso ? f + (size_t)6 * sim->np : nullptr;
+  tail = static_cast<char*>(sim->d_render) + core;
+  return PM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pm_status pm_density_grid(pm_sim* sim, float a, float b, float iso, int test_all_filled, int device_ptrs,
+                          uint32_t* M, uint32_t* M2, uint32_t* M4, uint32_t* cell_count, uint32_t* cell_offset,
+                          uint32_t* ids, uint32_t dims[3], double origin[3], double* voxel_size,
+                          uint32_t occupancy[2]) {
+  if (!sim || !dims) return fail(PM_ERR_INVALID, "NULL argument");
+  if (!sim->prepared) return fail(PM_ERR_STATE, "call pm_prepare first");
+  CK(cudaSetDevice(sim->device));
+  pm_status st = sim->sync_ctrl();
+  if (st != PM_OK) return st;
+  const DensityGeom g = density_geom(sim);
+  for (int d = 0; d < 3; ++d) {
+    dims[d] = (uint32_t)g.dims[d];
+    if (origin) origin[d] = g.start[d];
+  }
+  if (voxel_size) *voxel_size = g.h;
+  if (!M) return PM_OK;  // size query
+  const size_t X = g.dims[0], Y = g.dims[1], Z = g.dims[2];
+  const size_t ncell = X * Y * Z;
+  if (ncell > (size_t)4096 * 4096) return fail(PM_ERR_CAPACITY, "more density voxels than the binning scan covers");
+  const size_t n2 = ((X + 1) / 2) * ((Y + 1) / 2) * ((Z + 1) / 2), n4 = ((X + 3) / 4) * ((Y + 3) / 4) * ((Z + 3) / 4);
+  // staging: M2 / M4 always (a caller may not want them), M and ids for host outputs
+  const size_t staged = 4 * (n2 + n4) + (device_ptrs ? 0 : 4 * (ncell + (size_t)sim->np));
+  RenderScratch r{};
+  char* tail = nullptr;
+  if ((st = render_scratch(sim, (uint32_t)ncell, false, staged, r, tail)) != PM_OK) return st;
+  uint32_t* u = reinterpret_cast<uint32_t*>(tail);
+  uint32_t *dM = M, *dM2 = u, *dM4 = u + n2, *dids = ids;
+  if (device_ptrs) {
+    if (M2) dM2 = M2;
+    if (M4) dM4 = M4;
+  } else {
+    dM = u + n2 + n4;
+    dids = u + n2 + n4 + ncell;
+  }
+  Params p = sim->P;
+  cudaError_t e = launch_bin_particles(p, sim->d_pbuf[sim->cur], g, r, sim->stream);
+  const float kern = (float)(315.0 / (64.0 * M_PI * std::pow((double)g.h, 3)));  // BinaryDensityGrid.cpp:117
+  if (e == cudaSuccess)
+    e = launch_density_mask(g, r, a, b, kern, iso, test_all_filled, dM, dM2, dM4, sim->stream);
+  if (e == cudaSuccess && ids) e = launch_ids_to_pid(r.ids, sim->d_meta[sim->cur], r.misc, dids, (int)sim->np, sim->stream);
+  uint32_t misc[4] = {0, 0, 0, 0};
+  const cudaMemcpyKind k = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (e == cudaSuccess && cell_count) e = cudaMemcpyAsync(cell_count, r.counts, 4 * ncell, k, sim->stream);
+  if (e == cudaSuccess && cell_offset) e = cudaMemcpyAsync(cell_offset, r.offsets, 4 * ncell, k, sim->stream);
+  if (e == cudaSuccess && !device_ptrs) {
+    e = cudaMemcpyAsync(M, dM, 4 * ncell, cudaMemcpyDeviceToHost, sim->stream);
+    if (e == cudaSuccess && M2) e = cudaMemcpyAsync(M2, dM2, 4 * n2, cudaMemcpyDeviceToHost, sim->stream);
+    if (e == cudaSuccess && M4) e = cudaMemcpyAsync(M4, dM4, 4 * n4, cudaMemcpyDeviceToHost, sim->stream);
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(misc, r.misc, sizeof(misc), cudaMemcpyDeviceToHost, sim->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(sim->stream);
+  if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("density grid: ") + cudaGetErrorString(e));
+  if (ids && !device_ptrs) {
+    CK(cudaMemcpy(ids, dids, 4 * (size_t)misc[0], cudaMemcpyDeviceToHost));
+  }
+  if (occupancy) {
+    occupancy[0] = (uint32_t)(ncell - misc[1]);
+    occupancy[1] = misc[1];
+  }
+  return PM_OK;
+}
+
+pm_status pm_anisotropy(pm_sim* sim, float s, float k, int threshold, int auto_scale, int is_ani, float iso,
+                        int device_ptrs, float* G, float* G_inv, float* det, float* density, uint32_t* n_aggregate) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (!sim->prepared) return fail(PM_ERR_STATE, "call pm_prepare first");
+  if (!(k > 0.f)) return fail(PM_ERR_INVALID, "k must be positive");
+  CK(cudaSetDevice(sim->device));
+  pm_status st = sim->sync_ctrl();
+  if (st != PM_OK) return st;
+  const DensityGeom g = density_geom(sim);
+  const size_t ncell = (size_t)g.dims[0] * g.dims[1] * g.dims[2];
+  if (ncell > (size_t)4096 * 4096) return fail(PM_ERR_CAPACITY, "more density voxels than the binning scan covers");
+  const size_t np = sim->np;
+  const size_t staged = device_ptrs ? 0 : 4 * np * ((G ? 9 : 0) + (G_inv ? 9 : 0) + (det ? 1 : 0) + (density ? 1 : 0));
+  RenderScratch r{};
+  char* tail = nullptr;
+  if ((st = render_scratch(sim, (uint32_t)ncell, true, staged, r, tail)) != PM_OK) return st;
+  float *dG = G, *dGi = G_inv, *dD = det, *dR = density;
+  if (!device_ptrs) {
+    float* f = reinterpret_cast<float*>(tail);
+    if (G) { dG = f; f += 9 * np; }
+    if (G_inv) { dGi = f; f += 9 * np; }
+    if (det) { dD = f; f += np; }
+    if (density) { dR = f; f += np; }
+  }
+  AnisoParams ap{};
+  ap.s = s;
+  ap.k = k;
+  ap.threshold = threshold;
+  ap.auto_scale = auto_scale;
+  ap.is_ani = is_ani;
+  const float kern = 315.0f / (64.0f * (float)M_PI);  // state.h:36
+  Params p = sim->P;
+  cudaError_t e = launch_bin_particles(p, sim->d_pbuf[sim->cur], g, r, sim->stream);
+  if (e == cudaSuccess)
+    e = launch_anisotropy(p, sim->d_pbuf[sim->cur], sim->d_meta[sim->cur], g, r, ap, kern, iso, dG, dGi, dD, dR,
+                          sim->stream);
+  if (e == cudaSuccess && !device_ptrs) {
+    if (G) e = cudaMemcpyAsync(G, dG, 36 * np, cudaMemcpyDeviceToHost, sim->stream);
+    if (e == cudaSuccess && G_inv) e = cudaMemcpyAsync(G_inv, dGi, 36 * np, cudaMemcpyDeviceToHost, sim->stream);
+    if (e == cudaSuccess && det) e = cudaMemcpyAsync(det, dD, 4 * np, cudaMemcpyDeviceToHost, sim->stream);
+    if (e == cudaSuccess && density) e = cudaMemcpyAsync(density, dR, 4 * np, cudaMemcpyDeviceToHost, sim->stream);
+  }
+  uint32_t misc[4] = {0, 0, 0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(misc, r.misc, sizeof(misc), cudaMemcpyDeviceToHost, sim->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(sim->stream);
+  if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("anisotropy: ") + cudaGetErrorString(e));
+  if (n_aggregate) *n_aggregate = misc[2];
   return PM_OK;
 }
 

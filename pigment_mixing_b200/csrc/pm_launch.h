@@ -41,6 +41,38 @@ struct SplatGeom {
 // Two-pass splat into out[dims z][y][x][8] (latent 7 + weight); tmp: same size, pass-1 grid.
 cudaError_t launch_splat(const Params& P, const float* pcur, const uint32_t* meta, const float* G, const SplatGeom& g,
                          float* tmp, float* out, cudaStream_t s);
+// Density voxels of the renderer (AABBc::fixedAABB): origin, side h (the support radius) and counts.
+struct DensityGeom {
+  float start[3];
+  float h;
+  int dims[3];
+};
+// Classification::countMatrix parameters: covariance scale, eigenvalue clamp ratio, minimum
+// neighbour count, determinant rescaling (autoScaleS / !isAni).
+struct AnisoParams {
+  double s, k;
+  int threshold;
+  int auto_scale, is_ani;
+};
+// Scratch of the binning and anisotropy passes (render_scratch_bytes bytes, carved by the caller):
+// voxel counts and exclusive offsets, scan block sums, misc[0] binned total / [1] occupied voxels /
+// [2] aggregate particles, per sorted particle its voxel and rank, the binned sorted indices by
+// voxel, and (anisotropy) the symmetric matrices xx yy zz xy xz yz field-major with |det|.
+struct RenderScratch {
+  uint32_t *counts, *offsets, *bsum, *misc, *cellid, *rank, *ids;
+  float *Gs, *dets;
+};
+size_t render_scratch_bytes(uint32_t np, uint32_t ncell, bool aniso);
+cudaError_t launch_bin_particles(const Params& P, const float* pcur, const DensityGeom& g, RenderScratch& r,
+                                 cudaStream_t s);
+cudaError_t launch_density_mask(const DensityGeom& g, const RenderScratch& r, float wa, float wb, float kern, float iso,
+                                int test_all, uint32_t* M, uint32_t* M2, uint32_t* M4, cudaStream_t s);
+// ids (binned sorted indices, total[0] of them) -> particle indices
+cudaError_t launch_ids_to_pid(const uint32_t* ids, const uint32_t* meta, const uint32_t* total, uint32_t* out, int np,
+                              cudaStream_t s);
+cudaError_t launch_anisotropy(const Params& P, const float* pcur, const uint32_t* meta, const DensityGeom& g,
+                              const RenderScratch& r, const AnisoParams& ap, float kern, float iso, float* G,
+                              float* Ginv, float* det, float* density, cudaStream_t s);
 // Poisson-disk dart throwing into a background grid of nx*ny*nz cells of side cs (= r / sqrt(3)):
 // cells[c] = (x, y, z, 1) for a cell holding a sample, 0 otherwise.
 cudaError_t poisson_fill(float4* cells, int nx, int ny, int nz, float cs, float r, uint32_t seed, uint32_t passes,

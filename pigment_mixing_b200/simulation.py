@@ -56,6 +56,7 @@ class Simulation:
         call("pm_create", device, C.byref(h))
         self._h = h
         self._np = 0
+        self.device = device
 
     def close(self):
         if getattr(self, "_h", None):
@@ -305,6 +306,59 @@ class Simulation:
         call("pm_splat_pigments", self._h, None if g is None else g.ctypes.data_as(C.c_void_p), 0, sigma_spatial,
              sigma_color, vox.ctypes.data_as(C.c_void_p), up, _dp(origin), C.byref(vs))
         return vox, origin, vs.value
+
+    def densityGrid(self, a: float = 0.75, b: float = 0.74, iso: float = 9285.0, test_all_filled: bool = False) -> dict:
+        """The renderer's binary density grid (BinaryDensityGrid::fillBDG) over the density voxels
+        (side 2 dx): occupancy M and its 2^3 / 4^3 ORs M2 / M4 (voxel order x + X (y + Y z)), the
+        per-voxel particle counts and offsets, the binned particle indices grouped by voxel, and
+        the (empty, occupied) voxel counts."""
+        dims = np.zeros(3, np.uint32)
+        origin = np.zeros(3)
+        vs = C.c_double()
+        up = dims.ctypes.data_as(C.POINTER(C.c_uint32))
+        call("pm_density_grid", self._h, a, b, iso, int(test_all_filled), 0, None, None, None, None, None, None, up,
+             _dp(origin), C.byref(vs), None)
+        X, Y, Z = (int(v) for v in dims)
+        n = X * Y * Z
+        M = np.zeros(n, np.uint32)
+        M2 = np.zeros(((X + 1) // 2) * ((Y + 1) // 2) * ((Z + 1) // 2), np.uint32)
+        M4 = np.zeros(((X + 3) // 4) * ((Y + 3) // 4) * ((Z + 3) // 4), np.uint32)
+        counts, offsets = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        ids = np.zeros(self.Np, np.uint32)
+        occ = np.zeros(2, np.uint32)
+        vp = lambda a_: a_.ctypes.data_as(C.c_void_p)  # noqa: E731
+        call("pm_density_grid", self._h, a, b, iso, int(test_all_filled), 0, vp(M), vp(M2), vp(M4), vp(counts),
+             vp(offsets), vp(ids), up, _dp(origin), C.byref(vs), occ.ctypes.data_as(C.POINTER(C.c_uint32)))
+        return dict(M=M, M2=M2, M4=M4, counts=counts, offsets=offsets, ids=ids[:int(counts.sum())], dims=dims.copy(),
+                    origin=origin, voxel_size=vs.value, occupancy=(int(occ[0]), int(occ[1])))
+
+    def anisotropy(self, s: float = 1400.0, k: float = 4.0, threshold: int = 15, auto_scale: bool = True,
+                   is_ani: bool = True, iso: float = 9285.0, device: bool = False) -> dict:
+        """The renderer's per-particle anisotropy matrices G (n x 3 x 3, symmetric), their inverses,
+        |det G| and anisotropic densities (Classification::countDensities), original particle
+        order, and the count of aggregate particles (density > iso).  device=True returns torch
+        tensors on the simulation's GPU (G ready for splatPigments(G=..., out=...))."""
+        n = self.Np
+        agg = C.c_uint32()
+        if device:
+            import torch
+            dev = f"cuda:{self.device}"
+            G = torch.empty((n, 3, 3), dtype=torch.float32, device=dev)
+            Gi = torch.empty((n, 3, 3), dtype=torch.float32, device=dev)
+            det = torch.empty(n, dtype=torch.float32, device=dev)
+            dens = torch.empty(n, dtype=torch.float32, device=dev)
+            ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+            call("pm_anisotropy", self._h, s, k, threshold, int(auto_scale), int(is_ani), iso, 1, ptr(G), ptr(Gi),
+                 ptr(det), ptr(dens), C.byref(agg))
+        else:
+            G = np.zeros((n, 3, 3), np.float32)
+            Gi = np.zeros((n, 3, 3), np.float32)
+            det = np.zeros(n, np.float32)
+            dens = np.zeros(n, np.float32)
+            ptr = lambda a_: a_.ctypes.data_as(C.c_void_p)  # noqa: E731
+            call("pm_anisotropy", self._h, s, k, threshold, int(auto_scale), int(is_ani), iso, 0, ptr(G), ptr(Gi),
+                 ptr(det), ptr(dens), C.byref(agg))
+        return dict(G=G, G_inv=Gi, det=det, density=dens, n_aggregate=int(agg.value))
 
     def saveCheckpoint(self, path: str) -> None:
         call("pm_save_checkpoint", self._h, path.encode())
