@@ -565,7 +565,30 @@ def _splat_leg(scene, args, device, dist, with_cpu: bool):
     n = len(scene["x"])
     res = {"particles": n, "voxels": int(np.prod(vox0.shape[:3])), "voxel_size": vs, "ms": ms,
            "particles_per_s": n / (ms / 1e3), "sigma_spatial": 0.5, "sigma_color": 0.2,
-           "includes": "allocation of the two 8-float voxel grids, both passes and normalisations; no host copy"}
+           "includes": "both passes and normalisations into a device buffer (scratch grids kept between calls); "
+                       "no host copy"}
+    # the renderer's per-frame preprocessing before the splat: binary density grid, anisotropy
+    # matrices and densities, then the splat with those matrices (all device outputs)
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize(device)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize(device)
+        return _max_over_ranks(dist, a.elapsed_time(b) / reps, device)
+    bdg = g.densityGrid(device=True)
+    an = g.anisotropy(device=True)
+    res["density_grid"] = {"ms": timed(lambda: g.densityGrid(device=True)),
+                           "voxels": int(np.prod(bdg["dims"])), "occupied": bdg["occupancy"][1],
+                           "includes": "binning, filter, occupancy and its 2^3 / 4^3 ORs into device buffers"}
+    ams = timed(lambda: g.anisotropy(device=True))
+    res["anisotropy"] = {"ms": ams, "particles_per_s": n / (ams / 1e3), "n_aggregate": an["n_aggregate"],
+                         "includes": "binning, per-particle matrices, inverses, determinants and densities "
+                                     "into device buffers"}
+    res["splat_anisotropic_ms"] = timed(lambda: g.splatPigments(0.5, 0.2, G=an["G"], out=out))
     if with_cpu:
         from oracle import splat_ref
         st = g.getParticles(fields=("x", "latent"))
@@ -576,6 +599,16 @@ def _splat_leg(scene, args, device, dist, with_cpu: bool):
         el = time.perf_counter() - t0
         res["cpu_baseline"] = {"value": k / el, "unit": "particles/s", "cores": 1, "kind": "port",
                                "sample": f"first {k} particles, numpy restatement of both passes"}
+        from oracle import density_ref
+        # a compact piece of the body: the particles within 4 dx of the centre of mass
+        dxs = scene["params"]["dx"]
+        sel = np.all(np.abs(st.x - st.x.mean(0)) < 4 * dxs, axis=1)
+        t0 = time.perf_counter()
+        density_ref.anisotropy(st.x[sel], lo, hi, dxs)
+        el = time.perf_counter() - t0
+        res["anisotropy"]["cpu_baseline"] = {"value": int(sel.sum()) / el, "unit": "particles/s", "cores": 1,
+                                             "kind": "port", "sample": f"{int(sel.sum())} particles within 4 dx of "
+                                             "the centre of mass, numpy restatement"}
     g.close()
     return res
 

@@ -307,11 +307,13 @@ class Simulation:
              sigma_color, vox.ctypes.data_as(C.c_void_p), up, _dp(origin), C.byref(vs))
         return vox, origin, vs.value
 
-    def densityGrid(self, a: float = 0.75, b: float = 0.74, iso: float = 9285.0, test_all_filled: bool = False) -> dict:
+    def densityGrid(self, a: float = 0.75, b: float = 0.74, iso: float = 9285.0, test_all_filled: bool = False,
+                    device: bool = False) -> dict:
         """The renderer's binary density grid (BinaryDensityGrid::fillBDG) over the density voxels
         (side 2 dx): occupancy M and its 2^3 / 4^3 ORs M2 / M4 (voxel order x + X (y + Y z)), the
         per-voxel particle counts and offsets, the binned particle indices grouped by voxel, and
-        the (empty, occupied) voxel counts."""
+        the (empty, occupied) voxel counts.  device=True returns M, M2, M4 as torch tensors on
+        the simulation's GPU and skips the binning arrays."""
         dims = np.zeros(3, np.uint32)
         origin = np.zeros(3)
         vs = C.c_double()
@@ -320,6 +322,18 @@ class Simulation:
              _dp(origin), C.byref(vs), None)
         X, Y, Z = (int(v) for v in dims)
         n = X * Y * Z
+        if device:
+            import torch
+            dev = f"cuda:{self.device}"
+            M = torch.empty(n, dtype=torch.int32, device=dev)
+            M2 = torch.empty(((X + 1) // 2) * ((Y + 1) // 2) * ((Z + 1) // 2), dtype=torch.int32, device=dev)
+            M4 = torch.empty(((X + 3) // 4) * ((Y + 3) // 4) * ((Z + 3) // 4), dtype=torch.int32, device=dev)
+            occ = np.zeros(2, np.uint32)
+            ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+            call("pm_density_grid", self._h, a, b, iso, int(test_all_filled), 1, ptr(M), ptr(M2), ptr(M4), None, None,
+                 None, up, _dp(origin), C.byref(vs), occ.ctypes.data_as(C.POINTER(C.c_uint32)))
+            return dict(M=M, M2=M2, M4=M4, dims=dims.copy(), origin=origin, voxel_size=vs.value,
+                        occupancy=(int(occ[0]), int(occ[1])))
         M = np.zeros(n, np.uint32)
         M2 = np.zeros(((X + 1) // 2) * ((Y + 1) // 2) * ((Z + 1) // 2), np.uint32)
         M4 = np.zeros(((X + 3) // 4) * ((Y + 3) // 4) * ((Z + 3) // 4), np.uint32)

@@ -112,6 +112,9 @@ def test_density_grid_matches_restatement():
     for v in np.nonzero(ref["counts"])[0][:200]:
         o, n = ref["offsets"][v], ref["counts"][v]
         assert set(got["ids"][o:o + n]) == set(ref["ids"][o:o + n])
+    dev = g.densityGrid(device=True)
+    assert np.array_equal(dev["M"].cpu().numpy().astype(np.uint32), ref["M"])
+    assert np.array_equal(dev["M4"].cpu().numpy().astype(np.uint32), ref["M4"])
     # a lower iso threshold occupies more voxels; test-all-filled occupies all
     assert g.densityGrid(iso=1.0)["occupancy"][1] >= got["occupancy"][1]
     assert g.densityGrid(test_all_filled=True)["M"].all()
