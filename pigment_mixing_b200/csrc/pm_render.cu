@@ -21,10 +21,10 @@
 // The density of a particle is sum_j 315/(64 pi) |det G_j| (1 - |G_j (x_i - x_j)|^2)^3 over the
 // neighbours with |G_j (x_i - x_j)| <= 1.
 //
-// Layout: one thread per particle in the simulation's sorted order (neighbouring threads hold
-// neighbouring particles, so their neighbour loads hit the same cache lines); one thread per
-// density voxel for the occupancy grid.  The symmetric eigenproblem is solved in FP64 by cyclic
-// Jacobi rotations.
+// Layout: one thread per density voxel for the occupancy grid.  The anisotropy and density passes
+// run one CTA per voxel: the voxel's particles share one neighbourhood, staged once in shared
+// memory and tested by all threads in lockstep; particles outside the voxels (not binned) take a
+// per-thread path.  The symmetric eigenproblem is solved in FP64 by cyclic Jacobi rotations.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -266,117 +266,316 @@ __device__ void sym_eig3(double a00, double a11, double a22, double a01, double 
   l[2] = A[2][2];
 }
 
-__global__ void k_aniso(Params P, const float* __restrict__ pcur, const uint32_t* __restrict__ meta, DensityGeom g,
-                        const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
-                        const uint32_t* __restrict__ ids, AnisoParams ap, float* __restrict__ Gs,
-                        float* __restrict__ dets, float* G_out, float* Ginv_out, float* det_out) {
-  const int S = P.np_stride, np = P.np;
-  const float h = g.h;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
-    const float xi[3] = {pcur[(F_X + 0) * S + i], pcur[(F_X + 1) * S + i], pcur[(F_X + 2) * S + i]};
-    // one pass over the neighbours: weight sum, weighted mean and second moment of u = x_j - x_i
-    // (relative to the particle, so the covariance loses no digits to the absolute position)
-    uint32_t cnt = 0;
-    float ws = 0.f, su[3] = {0.f, 0.f, 0.f}, suu[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    const float ri = 2.f * h;
-    for_neighbours(g, pcur, S, counts, offsets, ids, xi, [&](uint32_t, const float d[3], float dd) {
-      const float q = sqrtf(dd) / ri;
-      const float om = 1.f - q;
-      const float w = om * om * om;
-      const float u[3] = {-d[0], -d[1], -d[2]};
-      ++cnt;
-      ws += w;
-      su[0] += w * u[0]; su[1] += w * u[1]; su[2] += w * u[2];
-      suu[0] += w * u[0] * u[0]; suu[1] += w * u[1] * u[1]; suu[2] += w * u[2] * u[2];
-      suu[3] += w * u[0] * u[1]; suu[4] += w * u[0] * u[2]; suu[5] += w * u[1] * u[2];
-    });
-    double B[6];  // xx yy zz xy xz yz
-    bool iso = cnt < (uint32_t)ap.threshold || ws < 1e-12f;
-    if (!iso) {
-      const double m[3] = {su[0] / (double)ws, su[1] / (double)ws, su[2] / (double)ws};
-      const double sc = ap.s / (double)ws;
-      const double c00 = sc * suu[0] - ap.s * m[0] * m[0], c11 = sc * suu[1] - ap.s * m[1] * m[1];
-      const double c22 = sc * suu[2] - ap.s * m[2] * m[2], c01 = sc * suu[3] - ap.s * m[0] * m[1];
-      const double c02 = sc * suu[4] - ap.s * m[0] * m[2], c12 = sc * suu[5] - ap.s * m[1] * m[2];
-      double l[3], V[9];
-      sym_eig3(c00, c11, c22, c01, c02, c12, l, V);
-      const double lmax = fmax(l[0], fmax(l[1], l[2]));
-      if (!(lmax > 0.0)) {
-        iso = true;  // no spread among the neighbours: keep the isotropic kernel
-      } else {
-        double e[3];
+// G, |det G| and G^-1 of one particle from its neighbour moments (Classification.cpp:60-100);
+// writes the sorted-order copies (Gs, dets) and the original-order outputs.
+__device__ void aniso_finish(int i, uint32_t pid, int np, float h, const AnisoParams& ap, uint32_t cnt, float ws,
+                             const float su[3], const float suu[6], float* __restrict__ Gs, float* __restrict__ dets,
+                             float* G_out, float* Ginv_out, float* det_out) {
+  double B[6];  // xx yy zz xy xz yz
+  bool iso = cnt < (uint32_t)ap.threshold || ws < 1e-12f;
+  if (!iso) {
+    const double m[3] = {su[0] / (double)ws, su[1] / (double)ws, su[2] / (double)ws};
+    const double sc = ap.s / (double)ws;
+    const double c00 = sc * suu[0] - ap.s * m[0] * m[0], c11 = sc * suu[1] - ap.s * m[1] * m[1];
+    const double c22 = sc * suu[2] - ap.s * m[2] * m[2], c01 = sc * suu[3] - ap.s * m[0] * m[1];
+    const double c02 = sc * suu[4] - ap.s * m[0] * m[2], c12 = sc * suu[5] - ap.s * m[1] * m[2];
+    double l[3], V[9];
+    sym_eig3(c00, c11, c22, c01, c02, c12, l, V);
+    const double lmax = fmax(l[0], fmax(l[1], l[2]));
+    if (!(lmax > 0.0)) {
+      iso = true;  // no spread among the neighbours: keep the isotropic kernel
+    } else {
+      double e[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) e[k] = 1.0 / sqrt(fmax(l[k], lmax / ap.k));
-        auto Bm = [&](int r, int q) {
-          return (V[3 * r] * e[0] * V[3 * q] + V[3 * r + 1] * e[1] * V[3 * q + 1] + V[3 * r + 2] * e[2] * V[3 * q + 2]) / h;
-        };
-        B[0] = Bm(0, 0); B[1] = Bm(1, 1); B[2] = Bm(2, 2); B[3] = Bm(0, 1); B[4] = Bm(0, 2); B[5] = Bm(1, 2);
-        if (ap.auto_scale || !ap.is_ani) {
-          const double det = fabs(B[0] * (B[1] * B[2] - B[5] * B[5]) - B[3] * (B[3] * B[2] - B[5] * B[4]) +
-                                  B[4] * (B[3] * B[5] - B[1] * B[4]));
-          if (det > 0.0) {
-            const double s3 = cbrt((1.0 / ((double)h * h * h)) / det);
+      for (int k = 0; k < 3; ++k) e[k] = 1.0 / sqrt(fmax(l[k], lmax / ap.k));
+      auto Bm = [&](int r, int q) {
+        return (V[3 * r] * e[0] * V[3 * q] + V[3 * r + 1] * e[1] * V[3 * q + 1] + V[3 * r + 2] * e[2] * V[3 * q + 2]) / h;
+      };
+      B[0] = Bm(0, 0); B[1] = Bm(1, 1); B[2] = Bm(2, 2); B[3] = Bm(0, 1); B[4] = Bm(0, 2); B[5] = Bm(1, 2);
+      if (ap.auto_scale || !ap.is_ani) {
+        const double det = fabs(B[0] * (B[1] * B[2] - B[5] * B[5]) - B[3] * (B[3] * B[2] - B[5] * B[4]) +
+                                B[4] * (B[3] * B[5] - B[1] * B[4]));
+        if (det > 0.0) {
+          const double s3 = cbrt((1.0 / ((double)h * h * h)) / det);
 #pragma unroll
-            for (int k = 0; k < 6; ++k) B[k] *= s3;
-          }
+          for (int k = 0; k < 6; ++k) B[k] *= s3;
         }
       }
     }
-    if (iso) {
-      B[0] = B[1] = B[2] = 1.0 / h;
-      B[3] = B[4] = B[5] = 0.0;
-    }
-    float Bf[6];
+  }
+  if (iso) {
+    B[0] = B[1] = B[2] = 1.0 / h;
+    B[3] = B[4] = B[5] = 0.0;
+  }
+  float Bf[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) Bf[k] = (float)B[k];
-    // determinant and inverse of the rounded matrix
-    const double b0 = Bf[0], b1 = Bf[1], b2 = Bf[2], b3 = Bf[3], b4 = Bf[4], b5 = Bf[5];
-    const double k00 = b1 * b2 - b5 * b5, k01 = b4 * b5 - b3 * b2, k02 = b3 * b5 - b1 * b4;
-    const double det = b0 * k00 + b3 * k01 + b4 * k02;
+  for (int k = 0; k < 6; ++k) Bf[k] = (float)B[k];
+  // determinant and inverse of the rounded matrix
+  const double b0 = Bf[0], b1 = Bf[1], b2 = Bf[2], b3 = Bf[3], b4 = Bf[4], b5 = Bf[5];
+  const double k00 = b1 * b2 - b5 * b5, k01 = b4 * b5 - b3 * b2, k02 = b3 * b5 - b1 * b4;
+  const double det = b0 * k00 + b3 * k01 + b4 * k02;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) Gs[(size_t)k * np + i] = Bf[k];
-    dets[i] = (float)fabs(det);
-    const uint32_t pid = meta[i] & ~kInactiveBit;
-    if (G_out) {
-      float* o = G_out + (size_t)pid * 9;
-      o[0] = Bf[0]; o[1] = Bf[3]; o[2] = Bf[4];
-      o[3] = Bf[3]; o[4] = Bf[1]; o[5] = Bf[5];
-      o[6] = Bf[4]; o[7] = Bf[5]; o[8] = Bf[2];
-    }
-    if (det_out) det_out[pid] = (float)fabs(det);
-    if (Ginv_out) {
-      const double id = 1.0 / det;
-      const double k11 = b0 * b2 - b4 * b4, k12 = b3 * b4 - b0 * b5, k22 = b0 * b1 - b3 * b3;
-      float* o = Ginv_out + (size_t)pid * 9;
-      o[0] = (float)(k00 * id); o[1] = (float)(k01 * id); o[2] = (float)(k02 * id);
-      o[3] = (float)(k01 * id); o[4] = (float)(k11 * id); o[5] = (float)(k12 * id);
-      o[6] = (float)(k02 * id); o[7] = (float)(k12 * id); o[8] = (float)(k22 * id);
+  for (int k = 0; k < 6; ++k) Gs[(size_t)k * np + i] = Bf[k];
+  dets[i] = (float)fabs(det);
+  if (G_out) {
+    float* o = G_out + (size_t)pid * 9;
+    o[0] = Bf[0]; o[1] = Bf[3]; o[2] = Bf[4];
+    o[3] = Bf[3]; o[4] = Bf[1]; o[5] = Bf[5];
+    o[6] = Bf[4]; o[7] = Bf[5]; o[8] = Bf[2];
+  }
+  if (det_out) det_out[pid] = (float)fabs(det);
+  if (Ginv_out) {
+    const double id = 1.0 / det;
+    const double k11 = b0 * b2 - b4 * b4, k12 = b3 * b4 - b0 * b5, k22 = b0 * b1 - b3 * b3;
+    float* o = Ginv_out + (size_t)pid * 9;
+    o[0] = (float)(k00 * id); o[1] = (float)(k01 * id); o[2] = (float)(k02 * id);
+    o[3] = (float)(k01 * id); o[4] = (float)(k11 * id); o[5] = (float)(k12 * id);
+    o[6] = (float)(k02 * id); o[7] = (float)(k12 * id); o[8] = (float)(k22 * id);
+  }
+}
+
+// neighbour moments: count, weight sum, weighted first and second moments of u = x_j - x_i
+struct Moments {
+  uint32_t cnt = 0;
+  float ws = 0.f, su[3] = {0.f, 0.f, 0.f}, suu[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  __device__ __forceinline__ void add(const float d[3], float dd, float inv_ri) {
+    const float q = sqrtf(dd) * inv_ri;
+    const float om = 1.f - q;
+    const float w = om * om * om;
+    const float u[3] = {-d[0], -d[1], -d[2]};
+    ++cnt;
+    ws += w;
+    su[0] += w * u[0]; su[1] += w * u[1]; su[2] += w * u[2];
+    suu[0] += w * u[0] * u[0]; suu[1] += w * u[1] * u[1]; suu[2] += w * u[2] * u[2];
+    suu[3] += w * u[0] * u[1]; suu[4] += w * u[0] * u[2]; suu[5] += w * u[1] * u[2];
+  }
+};
+
+// Per-thread form, for the particles outside the density voxels (not binned, so not covered by
+// the voxel-parallel kernels): unbinned only.
+__global__ void k_aniso(Params P, const float* __restrict__ pcur, const uint32_t* __restrict__ meta, DensityGeom g,
+                        const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                        const uint32_t* __restrict__ ids, const uint32_t* __restrict__ cellid, AnisoParams ap,
+                        float* __restrict__ Gs, float* __restrict__ dets, float* G_out, float* Ginv_out,
+                        float* det_out) {
+  const int S = P.np_stride, np = P.np;
+  const float h = g.h, inv_ri = 1.f / (2.f * h);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    if (cellid[i] != 0xffffffffu) continue;
+    const float xi[3] = {pcur[(F_X + 0) * S + i], pcur[(F_X + 1) * S + i], pcur[(F_X + 2) * S + i]};
+    Moments m;
+    for_neighbours(g, pcur, S, counts, offsets, ids, xi, [&](uint32_t, const float d[3], float dd) { m.add(d, dd, inv_ri); });
+    aniso_finish(i, meta[i] & ~kInactiveBit, np, h, ap, m.cnt, m.ws, m.su, m.suu, Gs, dets, G_out, Ginv_out, det_out);
+  }
+}
+
+__device__ __forceinline__ float density_term(const float d[3], float b0, float b1, float b2, float b3, float b4,
+                                              float b5, float det, float kern) {
+  const float l0 = b0 * d[0] + b3 * d[1] + b4 * d[2];
+  const float l1 = b3 * d[0] + b1 * d[1] + b5 * d[2];
+  const float l2v = b4 * d[0] + b5 * d[1] + b2 * d[2];
+  const float l2 = l0 * l0 + l1 * l1 + l2v * l2v;
+  if (l2 > 1.f) return 0.f;
+  const float om = 1.f - l2;
+  return kern * det * (om * om * om);
+}
+
+// Per-thread density for the unbinned particles.
+__global__ void k_density(Params P, const float* __restrict__ pcur, const uint32_t* __restrict__ meta, DensityGeom g,
+                          const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                          const uint32_t* __restrict__ ids, const uint32_t* __restrict__ cellid,
+                          const float* __restrict__ Gs, const float* __restrict__ dets, float kern, float iso,
+                          float* dens_out, uint32_t* n_agg) {
+  const int S = P.np_stride, np = P.np;
+  uint32_t agg = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    if (cellid[i] != 0xffffffffu) continue;
+    const float xi[3] = {pcur[(F_X + 0) * S + i], pcur[(F_X + 1) * S + i], pcur[(F_X + 2) * S + i]};
+    float dens = 0.f;
+    for_neighbours(g, pcur, S, counts, offsets, ids, xi, [&](uint32_t j, const float d[3], float) {
+      dens += density_term(d, Gs[j], Gs[(size_t)np + j], Gs[2 * (size_t)np + j], Gs[3 * (size_t)np + j],
+                           Gs[4 * (size_t)np + j], Gs[5 * (size_t)np + j], dets[j], kern);
+    });
+    if (dens_out) dens_out[meta[i] & ~kInactiveBit] = dens;
+    if (dens > iso) ++agg;
+  }
+  const uint32_t a = __reduce_add_sync(0xffffffffu, agg);
+  if ((threadIdx.x & 31) == 0 && a) atomicAdd(n_agg, a);
+}
+
+
+// ---- voxel-parallel forms: one CTA per density voxel.  Its particles share one neighbourhood (the
+// 27 voxels around it), so the CTA stages the neighbourhood's candidates in shared memory once
+// and every thread tests its particle against the same candidate at the same time (broadcast
+// reads, no divergence in the candidate loop).  Candidates keep the reference's order: voxels
+// z, then y, then x, and the binning order inside a voxel.
+constexpr int kVoxThreads = 64;
+constexpr int kCandA = 1024;  // candidates per staged chunk: positions (16 B)
+constexpr int kCandD = 448;   // positions + matrices (48 B)
+
+struct VoxSegs {
+  int nseg;
+  uint32_t off[27];
+  uint32_t pre[28];  // exclusive prefix of the segment lengths; pre[nseg] = candidates
+};
+
+// warp 0 lists the clamped 27-voxel neighbourhood of voxel (vx, vy, vz) as segments of ids[]
+__device__ __forceinline__ void vox_segments(const DensityGeom& g, const uint32_t* __restrict__ counts,
+                                             const uint32_t* __restrict__ offsets, int vx, int vy, int vz,
+                                             VoxSegs& sg) {
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  const int x0 = max(0, vx - 1), x1 = min(g.dims[0] - 1, vx + 1);
+  const int y0 = max(0, vy - 1), y1 = min(g.dims[1] - 1, vy + 1);
+  const int z0 = max(0, vz - 1), z1 = min(g.dims[2] - 1, vz + 1);
+  const int nx = x1 - x0 + 1, ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+  const int nseg = nx * ny * nz;
+  uint32_t c = 0;
+  if (lane < nseg) {
+    const int sx = lane % nx, sy = (lane / nx) % ny, sz = lane / (nx * ny);
+    const uint32_t id = bdg_id(g, x0 + sx, y0 + sy, z0 + sz);
+    c = counts[id];
+    sg.off[lane] = offsets[id];
+  }
+  uint32_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane < nseg) sg.pre[lane + 1] = incl;
+  if (lane == 0) {
+    sg.pre[0] = 0;
+    sg.nseg = nseg;
+  }
+}
+
+// candidate kk of the staged neighbourhood -> its sorted particle index (s: running segment)
+__device__ __forceinline__ uint32_t vox_candidate(const VoxSegs& sg, const uint32_t* __restrict__ ids, uint32_t kk,
+                                                  int& s) {
+  while (sg.pre[s + 1] <= kk) ++s;
+  return ids[sg.off[s] + (kk - sg.pre[s])];
+}
+
+__global__ void __launch_bounds__(kVoxThreads) k_aniso_vox(Params P, const float* __restrict__ pcur,
+                                                           const uint32_t* __restrict__ meta, DensityGeom g,
+                                                           const uint32_t* __restrict__ counts,
+                                                           const uint32_t* __restrict__ offsets,
+                                                           const uint32_t* __restrict__ ids, AnisoParams ap,
+                                                           float* __restrict__ Gs, float* __restrict__ dets,
+                                                           float* G_out, float* Ginv_out, float* det_out) {
+  __shared__ VoxSegs sg;
+  __shared__ float4 cand[kCandA];
+  const int S = P.np_stride, np = P.np;
+  const float h = g.h, inv_ri = 1.f / (2.f * h), h2 = h * h;
+  const uint32_t nvox = (uint32_t)g.dims[0] * g.dims[1] * g.dims[2];
+  for (uint32_t v = blockIdx.x; v < nvox; v += gridDim.x) {
+    const uint32_t nv = counts[v];
+    if (nv == 0) continue;
+    const uint32_t ov = offsets[v];
+    const int vx = (int)(v % (uint32_t)g.dims[0]), vy = (int)((v / (uint32_t)g.dims[0]) % (uint32_t)g.dims[1]);
+    const int vz = (int)(v / ((uint32_t)g.dims[0] * g.dims[1]));
+    __syncthreads();  // the previous voxel's readers are done with sg and cand
+    vox_segments(g, counts, offsets, vx, vy, vz, sg);
+    __syncthreads();
+    const uint32_t T = sg.pre[sg.nseg];
+    for (uint32_t t0 = 0; t0 < nv; t0 += kVoxThreads) {
+      const bool mine = t0 + threadIdx.x < nv;
+      const uint32_t i = mine ? ids[ov + t0 + threadIdx.x] : 0u;
+      float xi[3] = {0.f, 0.f, 0.f};
+      if (mine) { xi[0] = pcur[(F_X + 0) * S + i]; xi[1] = pcur[(F_X + 1) * S + i]; xi[2] = pcur[(F_X + 2) * S + i]; }
+      Moments m;
+      for (uint32_t c0 = 0; c0 < T; c0 += kCandA) {
+        const uint32_t nc = min((uint32_t)kCandA, T - c0);
+        const bool staged = t0 > 0 && T <= (uint32_t)kCandA;  // whole neighbourhood still in place
+        if (!staged) {
+          __syncthreads();
+          int sgi = 0;
+          for (uint32_t k = threadIdx.x; k < nc; k += kVoxThreads) {
+            const uint32_t j = vox_candidate(sg, ids, c0 + k, sgi);
+            cand[k] = make_float4(pcur[(F_X + 0) * S + j], pcur[(F_X + 1) * S + j], pcur[(F_X + 2) * S + j], 0.f);
+          }
+          __syncthreads();
+        }
+        if (mine) {
+#pragma unroll 4
+          for (uint32_t k = 0; k < nc; ++k) {
+            const float4 c = cand[k];
+            const float d[3] = {xi[0] - c.x, xi[1] - c.y, xi[2] - c.z};
+            const float dd = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            if (dd <= h2) m.add(d, dd, inv_ri);
+          }
+        }
+      }
+      if (mine) aniso_finish((int)i, meta[i] & ~kInactiveBit, np, h, ap, m.cnt, m.ws, m.su, m.suu, Gs, dets, G_out,
+                             Ginv_out, det_out);
     }
   }
 }
 
-__global__ void k_density(Params P, const float* __restrict__ pcur, const uint32_t* __restrict__ meta, DensityGeom g,
-                          const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
-                          const uint32_t* __restrict__ ids, const float* __restrict__ Gs,
-                          const float* __restrict__ dets, float kern, float iso, float* dens_out, uint32_t* n_agg) {
+__global__ void __launch_bounds__(kVoxThreads) k_density_vox(Params P, const float* __restrict__ pcur,
+                                                             const uint32_t* __restrict__ meta, DensityGeom g,
+                                                             const uint32_t* __restrict__ counts,
+                                                             const uint32_t* __restrict__ offsets,
+                                                             const uint32_t* __restrict__ ids,
+                                                             const float* __restrict__ Gs,
+                                                             const float* __restrict__ dets, float kern, float iso,
+                                                             float* dens_out, uint32_t* n_agg) {
+  __shared__ VoxSegs sg;
+  __shared__ float4 cand[3 * kCandD];  // per candidate: x y z |det|, G xx yy zz xy, G xz yz - -
   const int S = P.np_stride, np = P.np;
+  const float h2 = g.h * g.h;
+  const uint32_t nvox = (uint32_t)g.dims[0] * g.dims[1] * g.dims[2];
   uint32_t agg = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
-    const float xi[3] = {pcur[(F_X + 0) * S + i], pcur[(F_X + 1) * S + i], pcur[(F_X + 2) * S + i]};
-    float dens = 0.f;
-    for_neighbours(g, pcur, S, counts, offsets, ids, xi, [&](uint32_t j, const float d[3], float) {
-      const float b0 = Gs[j], b1 = Gs[(size_t)np + j], b2 = Gs[2 * (size_t)np + j];
-      const float b3 = Gs[3 * (size_t)np + j], b4 = Gs[4 * (size_t)np + j], b5 = Gs[5 * (size_t)np + j];
-      const float l0 = b0 * d[0] + b3 * d[1] + b4 * d[2];
-      const float l1 = b3 * d[0] + b1 * d[1] + b5 * d[2];
-      const float l2v = b4 * d[0] + b5 * d[1] + b2 * d[2];
-      const float l2 = l0 * l0 + l1 * l1 + l2v * l2v;
-      if (l2 > 1.f) return;
-      const float om = 1.f - l2;
-      dens += kern * dets[j] * (om * om * om);
-    });
-    if (dens_out) dens_out[meta[i] & ~kInactiveBit] = dens;
-    if (dens > iso) ++agg;
+  for (uint32_t v = blockIdx.x; v < nvox; v += gridDim.x) {
+    const uint32_t nv = counts[v];
+    if (nv == 0) continue;
+    const uint32_t ov = offsets[v];
+    const int vx = (int)(v % (uint32_t)g.dims[0]), vy = (int)((v / (uint32_t)g.dims[0]) % (uint32_t)g.dims[1]);
+    const int vz = (int)(v / ((uint32_t)g.dims[0] * g.dims[1]));
+    __syncthreads();
+    vox_segments(g, counts, offsets, vx, vy, vz, sg);
+    __syncthreads();
+    const uint32_t T = sg.pre[sg.nseg];
+    for (uint32_t t0 = 0; t0 < nv; t0 += kVoxThreads) {
+      const bool mine = t0 + threadIdx.x < nv;
+      const uint32_t i = mine ? ids[ov + t0 + threadIdx.x] : 0u;
+      float xi[3] = {0.f, 0.f, 0.f};
+      if (mine) { xi[0] = pcur[(F_X + 0) * S + i]; xi[1] = pcur[(F_X + 1) * S + i]; xi[2] = pcur[(F_X + 2) * S + i]; }
+      float dens = 0.f;
+      for (uint32_t c0 = 0; c0 < T; c0 += kCandD) {
+        const uint32_t nc = min((uint32_t)kCandD, T - c0);
+        const bool staged = t0 > 0 && T <= (uint32_t)kCandD;
+        if (!staged) {
+          __syncthreads();
+          int sgi = 0;
+          for (uint32_t k = threadIdx.x; k < nc; k += kVoxThreads) {
+            const uint32_t j = vox_candidate(sg, ids, c0 + k, sgi);
+            cand[3 * k] = make_float4(pcur[(F_X + 0) * S + j], pcur[(F_X + 1) * S + j], pcur[(F_X + 2) * S + j],
+                                      dets[j]);
+            cand[3 * k + 1] = make_float4(Gs[j], Gs[(size_t)np + j], Gs[2 * (size_t)np + j], Gs[3 * (size_t)np + j]);
+            cand[3 * k + 2] = make_float4(Gs[4 * (size_t)np + j], Gs[5 * (size_t)np + j], 0.f, 0.f);
+          }
+          __syncthreads();
+        }
+        if (mine) {
+#pragma unroll 4
+          for (uint32_t k = 0; k < nc; ++k) {
+            const float4 c = cand[3 * k];
+            const float d[3] = {xi[0] - c.x, xi[1] - c.y, xi[2] - c.z};
+            const float dd = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            if (dd <= h2) {
+              const float4 b = cand[3 * k + 1], e = cand[3 * k + 2];
+              dens += density_term(d, b.x, b.y, b.z, b.w, e.x, e.y, c.w, kern);
+            }
+          }
+        }
+      }
+      if (mine) {
+        if (dens_out) dens_out[meta[i] & ~kInactiveBit] = dens;
+        if (dens > iso) ++agg;
+      }
+    }
   }
   const uint32_t a = __reduce_add_sync(0xffffffffu, agg);
   if ((threadIdx.x & 31) == 0 && a) atomicAdd(n_agg, a);
@@ -443,10 +642,17 @@ cudaError_t launch_anisotropy(const Params& P, const float* pcur, const uint32_t
                               const RenderScratch& r, const AnisoParams& ap, float kern, float iso, float* G,
                               float* Ginv, float* det, float* density, cudaStream_t s) {
   if (P.np <= 0) return cudaSuccess;
-  k_aniso<<<grid_for(P.np, 8), kRenderThreads, 0, s>>>(P, pcur, meta, g, r.counts, r.offsets, r.ids, ap, r.Gs, r.dets,
-                                                      G, Ginv, det);
-  k_density<<<grid_for(P.np, 8), kRenderThreads, 0, s>>>(P, pcur, meta, g, r.counts, r.offsets, r.ids, r.Gs, r.dets,
-                                                        kern, iso, density, r.misc + 2);
+  const int sms = num_sms() > 0 ? num_sms() : 148;
+  const long long nvox = (long long)g.dims[0] * g.dims[1] * g.dims[2];
+  const int vgrid = (int)(nvox < (long long)sms * 16 ? nvox : (long long)sms * 16);
+  k_aniso_vox<<<vgrid, kVoxThreads, 0, s>>>(P, pcur, meta, g, r.counts, r.offsets, r.ids, ap, r.Gs, r.dets, G, Ginv,
+                                            det);
+  k_aniso<<<grid_for(P.np, 8), kRenderThreads, 0, s>>>(P, pcur, meta, g, r.counts, r.offsets, r.ids, r.cellid, ap,
+                                                      r.Gs, r.dets, G, Ginv, det);
+  k_density_vox<<<vgrid, kVoxThreads, 0, s>>>(P, pcur, meta, g, r.counts, r.offsets, r.ids, r.Gs, r.dets, kern, iso,
+                                              density, r.misc + 2);
+  k_density<<<grid_for(P.np, 8), kRenderThreads, 0, s>>>(P, pcur, meta, g, r.counts, r.offsets, r.ids, r.cellid,
+                                                        r.Gs, r.dets, kern, iso, density, r.misc + 2);
   return cudaGetLastError();
 }
 
