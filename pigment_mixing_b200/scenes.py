@@ -2,8 +2,9 @@
 
 The reference builds its paint scene from OpenVDB blob level sets with Poisson-disk sampling
 (matter/src/simulation/simulation_blobs.cpp:7-150, 27 particles per cell); those assets and
-libraries are not used here.  These builders place cuboid paint blocks of 8 jittered particles
-per cell instead (2 x 2 x 2 sub-cells, uniform jitter inside each), all from a seed.
+libraries are not used here.  The measured workloads place cuboid paint blocks of 8 jittered
+particles per cell (2 x 2 x 2 sub-cells, uniform jitter inside each), all from a seed;
+``blob_scene`` restates the reference's blob recipe with analytic dome-shaped blobs.
 
 A scene is a plain dict that ``apply(scene, sim)`` loads into any object with the Simulation
 call surface (the product :class:`Simulation` or the CPU oracle).
@@ -211,6 +212,140 @@ def sample_particles(Lx: float, Ly: float, Lz: float, radius: float, ppc: float 
     call("pm_sample_particles", device, Lx, Ly, Lz, radius, ppc, crop_to_shape, attempts, passes, seed,
          x.ctypes.data_as(C.POINTER(C.c_float)), n.value, C.byref(n), C.byref(dx), C.byref(vol))
     return x, dx.value, vol.value
+
+
+# ---- blob scenes (Simulation::blobs, matter/src/simulation/simulation_blobs.cpp:7-150) ---------------
+# Volumes of the reference's blob ladder (simulation.hpp:272-279: Blob_01 ... Blob_06).
+BLOB_VOLUMES = (0.0056, 0.0151, 0.0246, 0.0341, 0.0436, 0.053)
+
+
+class DomeBlob:
+    """An analytic paint dab standing in for the reference's VDB blobs: the upper half of a
+    superellipsoid |dx/R|^p + |y/H|^p + |dz/R|^p <= 1 resting on y = 0, centred at (cx, cz)."""
+
+    def __init__(self, volume: float, aspect: float = 0.55, exponent: float = 2.5):
+        from math import gamma
+        self.p = float(exponent)
+        self.k = 4.0 * aspect * gamma(1.0 + 1.0 / self.p) ** 3 / gamma(1.0 + 3.0 / self.p)  # V = k R^3
+        self.R = (volume / self.k) ** (1.0 / 3.0)
+        self.H = aspect * self.R
+        self.c = np.zeros(3)
+
+    @property
+    def volume(self) -> float:
+        return self.k * self.R ** 3
+
+    def bounds(self):
+        lo = self.c + np.array([-self.R, 0.0, -self.R])
+        hi = self.c + np.array([self.R, self.H, self.R])
+        return lo, hi
+
+    def inside(self, x) -> np.ndarray:
+        d = np.asarray(x, np.float64) - self.c
+        f = (np.abs(d[:, 0]) / self.R) ** self.p + (np.abs(d[:, 1]) / self.H) ** self.p + \
+            (np.abs(d[:, 2]) / self.R) ** self.p
+        return (f <= 1.0) & (d[:, 1] >= 0.0)
+
+
+def blob_target_volume(ratio: float) -> float:
+    """Colour ratio -> blob volume: the ratio clamped to [0.1, 0.9] mapped linearly onto the
+    ladder's volume range (simulation_blobs.cpp:11-24)."""
+    lo, hi = BLOB_VOLUMES[0], BLOB_VOLUMES[-1]
+    r = min(0.9, max(0.1, float(ratio)))
+    return min(hi, max(lo, lo + (r - 0.1) / 0.8 * (hi - lo)))
+
+
+def blob_offsets(radii) -> np.ndarray:
+    """Ground-plane placement of n blobs of the given packing radii so that neighbours touch
+    (simulation_blobs.cpp:63-116): one at the origin; two side by side on x; three with the third
+    touching both; four in two rows of two; more in a row along x.  Returns n x 3 offsets (y 0),
+    centred on the x / z bounds of the arrangement (:118-140)."""
+    r = [float(v) for v in radii]
+    n = len(r)
+    o = np.zeros((n, 3))
+    if n == 2:
+        o[0, 0], o[1, 0] = -r[0], r[1]
+    elif n == 3:
+        o[1, 0] = r[0] + r[1]
+        x1 = o[1, 0]
+        x2 = ((r[0] + r[2]) ** 2 - (r[1] + r[2]) ** 2 + x1 * x1) / (2.0 * x1)
+        o[2, 0] = x2
+        o[2, 2] = np.sqrt(max(0.0, (r[0] + r[2]) ** 2 - x2 * x2))
+    elif n == 4:
+        o[0, 0], o[1, 0], o[2, 0], o[3, 0] = -r[0], r[1], -r[2], r[3]
+
+        def cz(d, dist):
+            return np.sqrt(max(0.0, dist * dist - d * d))
+        Z = max(cz(o[0, 0] - o[2, 0], r[0] + r[2]), cz(o[1, 0] - o[3, 0], r[1] + r[3]),
+                cz(o[0, 0] - o[3, 0], r[0] + r[3]), cz(o[1, 0] - o[2, 0], r[1] + r[2]))
+        o[2, 2] = o[3, 2] = Z
+    elif n > 4:
+        cur = 0.0
+        for i in range(n):
+            if i > 0:
+                cur += r[i - 1] + r[i]
+            o[i, 0] = cur
+    if n:
+        rr = np.asarray(r)
+        lo = np.min(o - rr[:, None], axis=0)
+        hi = np.max(o + rr[:, None], axis=0)
+        centre = 0.5 * (lo + hi)
+        centre[1] = 0.0
+        o = o - centre
+    return o
+
+
+def blob_scene(color_ratios, latents=None, radius: float = 0.01, ppc: float = 27.0, seed: int = 42,
+               aspect: float = 0.55, exponent: float = 2.5, material: str = "dpvisc", knife: bool = True,
+               steps: int = 500, device: int = 0) -> dict:
+    """The reference's paint scene (Simulation::blobs): one blob per colour ratio, sized by
+    blob_target_volume, packed by blob_offsets around (0.5, 0, 0.5), filled by Poisson-disk
+    sampling of each blob's bounding box (pm_sample_particles, radius `radius`, 30 attempts, seed
+    seed + i) kept inside the blob, and dx = cbrt(ppc * sum of box volumes / sum of box samples)
+    (sampleParticlesFromVdb, sampling_particles_vdb.hpp:87-150).  The blobs are analytic domes
+    (DomeBlob) instead of the reference's VDB level sets; their packing radius is the exact
+    footprint radius, where the reference subtracts 0.055 from its padded VDB bounds."""
+    n = len(color_ratios)
+    if latents is None:
+        latents = [MIXBOX_LATENTS[RGB_SEEDS[i % len(RGB_SEEDS)]] for i in range(n)]
+    blobs = [DomeBlob(blob_target_volume(c), aspect, exponent) for c in color_ratios]
+    off = blob_offsets([b.R for b in blobs])
+    for b, o in zip(blobs, off):
+        b.c = o + np.array([0.5, 0.0, 0.5])
+    xs, lats = [], []
+    total_vol, total_samples = 0.0, 0
+    for i, b in enumerate(blobs):
+        lo, hi = b.bounds()
+        L = hi - lo
+        pts, _, _ = sample_particles(L[0], L[1], L[2], radius, ppc, 0, 30, 2, seed + i, device)
+        pts = pts.astype(np.float64) + lo
+        total_vol += float(np.prod(L))
+        total_samples += len(pts)
+        keep = pts[b.inside(pts)]
+        xs.append(keep.astype(np.float32))
+        lats.append(np.tile(np.asarray(latents[i % len(latents)], np.float32), (len(keep), 1)))
+    x = np.concatenate(xs)
+    dx = float(np.cbrt(ppc / total_samples * total_vol))
+    sc = two_block_scene(dx, (1, 1, 1), seed=seed, steps=steps, knife=False, material=material)
+    sc["x"], sc["latent"] = x, np.concatenate(lats)
+    p = sc["params"]
+    p["dx"] = dx
+    p["particle_volume"] = dx ** 3 / ppc
+    p["particle_mass"] = p["rho"] * p["particle_volume"]
+    lo = np.min([b.bounds()[0] for b in blobs], axis=0)
+    hi = np.max([b.bounds()[1] for b in blobs], axis=0)
+    margin = 0.25
+    sc["vectors"]["particle_boundary_min"] = [float(lo[0] - margin), 0.0, float(lo[2] - margin)]
+    sc["vectors"]["particle_boundary_max"] = [float(hi[0] + margin), float(hi[1] + margin), float(hi[2] + margin)]
+    if knife:
+        rng = np.random.default_rng(seed)
+        half = [0.2, 0.1, 0.005]
+        path = knife_path(rng, 0.5, half[1] + 0.5 * dx, lo[2] - 0.05, hi[2] + 0.05)
+        sc["objects"].append(("box_knife", dict(bc=2, friction=0.3, half=half, waypoints=path, speed=0.5)))
+    sc["blobs"] = [dict(centre=b.c.tolist(), R=b.R, H=b.H, volume=b.volume, particles=len(xx))
+                   for b, xx in zip(blobs, xs)]
+    sc["name"] = f"blobs_{n}"
+    return sc
 
 
 def apply(scene: dict, sim) -> None:
