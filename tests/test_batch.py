@@ -138,7 +138,7 @@ def test_batch_autotune_and_profile():
     steps = [m.steps_done for m in members]
     assert len(set(steps)) == 1 and steps[0] > 0  # autotuning advances all scenes alike
     prof = b.profile(2)
-    assert "kb_p2g" in prof and "kb_defgrad" in prof and len(prof) == b.kernels_per_round
+    assert "kb_p2g" in prof and "kb_defgrad_tail" in prof and len(prof) == b.kernels_per_round
     assert all(v >= 0.0 for v in prof.values())
     b.step(3)
     assert len({m.steps_done for m in members}) == 1
