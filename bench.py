@@ -39,8 +39,8 @@ ALGO_BYTES = {
     "k_g2p_musl": (144.0, 108.0),    # read x,v,latent + write v,B,latent,diff,pic ; read grid + MUSL grid
     # the deformation update runs as two kernels; their 72 B of F_trial round trip are not in
     # the reference's step structure, so they are not algorithmic bytes
-    "k_defgrad_head": (72.0, 12.0),  # read x,pic,F + write x ; read MUSL velocity
-    "k_defgrad_tail": (64.0, 0.0),   # read plastic + write F,plastic
+    "k_defgrad_head": (36.0, 12.0),  # read x,pic + write x ; read MUSL velocity
+    "k_defgrad_tail": (100.0, 0.0),  # read F,plastic + write F,plastic
     "k_grid_update": (0.0, 40.0),    # read 16 B, write v and flip 24 B per node
     "k_clear_bricks": (0.0, 80.0),   # zero the accumulated and MUSL records of touched bricks
 }

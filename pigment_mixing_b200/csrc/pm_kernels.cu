@@ -565,7 +565,10 @@ constexpr int kThreads = 128;  // threads per CTA of the brick kernels
 // is sized for (launch bounds): more CTAs hide more latency, fewer leave registers for the
 // FP64 SVD.
 #ifndef PM_DEFGRAD_MINB
-#define PM_DEFGRAD_MINB 8
+#define PM_DEFGRAD_MINB 7
+#endif
+#ifndef PM_HEAD_MINB
+#define PM_HEAD_MINB 8
 #endif
 #ifndef PM_G2P_MINB
 #define PM_G2P_MINB 7
@@ -1675,12 +1678,13 @@ __device__ __forceinline__ void finish_F_tau(const Params& P, const float* U, co
   tau[3] = T(0, 1); tau[4] = T(0, 2); tau[5] = T(1, 2);
 }
 
-// The update runs as two kernels.  kPart 1, the head, over the bricks: velocity gradient from the
-// brick's MUSL velocity tile, position update, F_trial = F + dt L F (FP64, stored as float in the F
-// field).  kPart 2, the tail, over the active particles in sorted order: F_trial read back, the
-// FP64 SVD, return map and stress.  Split this way the tail is a flat particle-parallel kernel
-// with no block barriers and a smaller instruction footprint than the whole update (on the 2M
-// scene 0.140 + 0.175 ms against 0.372 ms as one kernel, for 72 B more traffic per particle).
+// The update runs as two kernels.  kPart 1, the head, over the bricks: velocity gradient L from
+// the brick's MUSL velocity tile (handed to the tail in the output's F field) and the position
+// update.  kPart 2, the tail, over the active particles in sorted order: F_trial = F + dt L F in
+// FP64, the FP64 SVD, return map and stress.  Split this way the tail is a flat particle-parallel
+// kernel with no block barriers and a smaller instruction footprint than the whole update (on the
+// 2M scene 0.140 + 0.175 ms against 0.372 ms as one kernel, for 72 B more traffic per particle:
+// L out and back).
 template <int kModel, bool kExtras, int kPart>
 __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const int model = kModel >= 0 ? kModel : P.plastic_model;
@@ -1812,31 +1816,35 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
       maxv2 = fmaxf(maxv2, v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
       for (int r = 0; r < 3; ++r) { int k = fkey(xn[r]); mn[r] = min(mn[r], k); mx[r] = max(mx[r], k); }
     }
-    // F_trial = F + dt L F (FP64)
-    double F[9], Ft[9];
+    // the velocity gradient goes to the tail through the output's F field
 #pragma unroll
-    for (int k = 0; k < 9; ++k) F[k] = (double)pi[(F_F + k) * S + o];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        double s = 0.0;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) s += (double)L[3 * r + k] * F[3 * k + q];
-        Ft[3 * r + q] = F[3 * r + q] + dt * s;
-      }
-    // F_trial is the stored F unless the return map changes it (then it is overwritten below;
-    // both writes meet in L2), so it need not stay in registers across the SVD
-#pragma unroll
-    for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = (float)Ft[k];
+    for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = L[k];
   };
   if constexpr (kPart == 2) {
     const int nact_sorted = (int)B.cell[c->n_nodes];
     for (int i = blk_ * blockDim.x + threadIdx.x; i < nact_sorted; i += stride) {
-      double Ft[9];
+      const uint32_t o = B.sorted[i];
+      // F_trial = F + dt L F (FP64)
+      double L[9], F[9], Ft[9];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) Ft[k] = (double)po[(F_F + k) * S + i];
-      tail(i, B.sorted[i], Ft);
+      for (int k = 0; k < 9; ++k) {
+        L[k] = (double)po[(F_F + k) * S + i];
+        F[k] = (double)pi[(F_F + k) * S + o];
+      }
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          double sum = 0.0;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) sum += L[3 * r + k] * F[3 * k + q];
+          Ft[3 * r + q] = F[3 * r + q] + dt * sum;
+        }
+      // F_trial is the stored F unless the return map changes it (then it is overwritten in the
+      // tail; both writes meet in L2), so it need not stay in registers across the SVD
+#pragma unroll
+      for (int k = 0; k < 9; ++k) po[(F_F + k) * S + i] = (float)Ft[k];
+      tail(i, o, Ft);
     }
   }
   const int nbr = kPart == 2 ? 0 : c->n_bricks;
@@ -1912,14 +1920,14 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
 }
 // Plain-solver instantiations per plastic model (kExtras = false) and the generic kernel (model
 // and extras chosen at run time) that the surrogate, the sample log and mixed batches use.
-__global__ void __launch_bounds__(kThreads, 8) k_defgrad_head(Params P, Bufs B) {
+__global__ void __launch_bounds__(kThreads, PM_HEAD_MINB) k_defgrad_head(Params P, Bufs B) {
   d_defgrad<PL_NONE, false, 1>(P, B, blockIdx.x, gridDim.x);
 }
 template <int kModel, bool kExtras>
 __global__ void __launch_bounds__(kThreads, PM_DEFGRAD_MINB) k_defgrad_tail(Params P, Bufs B) {
   d_defgrad<kModel, kExtras, 2>(P, B, blockIdx.x, gridDim.x);
 }
-__global__ void __launch_bounds__(kThreads, 8) kb_defgrad_head(const SceneDev* __restrict__ sd,
+__global__ void __launch_bounds__(kThreads, PM_HEAD_MINB) kb_defgrad_head(const SceneDev* __restrict__ sd,
                                                                const int* __restrict__ off, int ns) {
   int s_, blk_, nblk_;
   batch_slot(off, ns, s_, blk_, nblk_);
@@ -2190,7 +2198,7 @@ void launch_step(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev
   {
     const int g = sms * g_occ_def;
     const bool extras = P.return_map == 1 || P.log_cap > 0;
-    k_defgrad_head<<<sms * 8, kThreads, 0, s>>>(P, B); mark();
+    k_defgrad_head<<<sms * PM_HEAD_MINB, kThreads, 0, s>>>(P, B); mark();
     if (!extras && P.plastic_model == PL_VMVISC) k_defgrad_tail<PL_VMVISC, false><<<g, kThreads, 0, s>>>(P, B);
     else if (!extras && P.plastic_model == PL_DPVISC) k_defgrad_tail<PL_DPVISC, false><<<g, kThreads, 0, s>>>(P, B);
     else if (!extras && P.plastic_model == PL_NONE) k_defgrad_tail<PL_NONE, false><<<g, kThreads, 0, s>>>(P, B);
