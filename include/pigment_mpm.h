@@ -255,6 +255,12 @@ PM_API pm_status pm_sample_particles(int device, double Lx, double Ly, double Lz
                                      int crop_to_shape, uint32_t attempts, uint32_t passes, uint32_t seed, float* x,
                                      uint32_t capacity, uint32_t* n, double* dx, double* particle_volume);
 
+/* ---- self-test of the device SVD --------------------------------------------------------------
+ * No counterpart in the reference (it calls Eigen's JacobiSVD, plasticity.cpp:18).  Runs the step's
+ * warm-started FP64 SVD on n host matrices A (row-major 3x3, FP64): A = U diag(S) V^T with S >= 0
+ * in FP64 and U, V rounded to FP32, as the return map uses them. */
+PM_API pm_status pm_svd3_batch(int device, const double* A, uint32_t n, float* U, double* S, float* V);
+
 /* ---- headless pigment splat --------------------------------------------------------------------
  * BinaryDensityGrid::fillRenderGrid (raytracing/src/raymarch/BinaryDensityGrid.cpp:153-296) without
  * the GL upload: the two-pass anisotropic bilateral splat of the particle latents onto the pigment

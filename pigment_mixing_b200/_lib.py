@@ -66,6 +66,7 @@ SIGNATURES = {
     "pm_save_checkpoint": [_vp, C.c_char_p],
     "pm_load_checkpoint": [_vp, C.c_char_p],
     "pm_splat_pigments": [_vp, _vp, C.c_int, C.c_float, C.c_float, _vp, _up, _dp, _dp],
+    "pm_svd3_batch": [C.c_int, _vp, C.c_uint32, _vp, _vp, _vp],
     "pm_density_grid": [_vp, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _up,
                         _dp, _dp, _up],
     "pm_anisotropy": [_vp, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _vp, _vp, _vp, _vp,

@@ -2251,6 +2251,35 @@ pm_status pm_anisotropy(pm_sim* sim, float s, float k, int threshold, int auto_s
 
 }  // extern "C"
 
+extern "C" pm_status pm_svd3_batch(int device, const double* A, uint32_t n, float* U, double* S, float* V) {
+  if (!A || !U || !S || !V) return fail(PM_ERR_INVALID, "NULL argument");
+  CK(cudaSetDevice(device));
+  cudaError_t e = cudaSuccess;
+  if (num_sms() <= 0 && (e = launch_init(device)) != cudaSuccess)
+    return fail(PM_ERR_CUDA, std::string("kernel set-up: ") + cudaGetErrorString(e));
+  if (n == 0) return PM_OK;
+  double *dA = nullptr, *dS = nullptr;
+  float *dU = nullptr, *dV = nullptr;
+  auto release = [&]() { cudaFree(dA); cudaFree(dS); cudaFree(dU); cudaFree(dV); };
+  if (cudaMalloc(&dA, 72ull * n) != cudaSuccess || cudaMalloc(&dS, 24ull * n) != cudaSuccess ||
+      cudaMalloc(&dU, 36ull * n) != cudaSuccess || cudaMalloc(&dV, 36ull * n) != cudaSuccess) {
+    release();
+    cudaGetLastError();
+    return fail(PM_ERR_CUDA, "allocation failed");
+  }
+  e = cudaMemcpy(dA, A, 72ull * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    launch_svd3_batch(dA, (int)n, dU, dS, dV, nullptr);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(U, dU, 36ull * n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(S, dS, 24ull * n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(V, dV, 36ull * n, cudaMemcpyDeviceToHost);
+  release();
+  if (e != cudaSuccess) return fail(PM_ERR_CUDA, std::string("svd self-test: ") + cudaGetErrorString(e));
+  return PM_OK;
+}
+
 // ------------------------------------------------------------------------------------------
 // Poisson-disk particle sampling (sampleParticles, sampling_particles.hpp:12-70)
 // ------------------------------------------------------------------------------------------

@@ -1333,6 +1333,11 @@ __device__ __forceinline__ void jrot_f32(float& app, float& aqq, float& apq, flo
 // accurate to first order: (cos, sin) are computed in FP32 from the FP64 column products and
 // renormalised in FP64 by one Newton step on cos^2 + sin^2 = 1 (error O(1e-14)), which replaces
 // the FP64 divide, square root and reciprocal square root of each rotation.
+// At most this many FP32 warm-start sweeps (the FP64 sweeps that follow converge regardless of
+// the start; on the 2M scene the tail measured 0.181 ms with 2, 0.187 with 3, 0.194 with 1 or 5).
+#ifndef PM_SVD_WARM_SWEEPS
+#define PM_SVD_WARM_SWEEPS 2
+#endif
 __device__ void svd3_warm(const double A[9], float Uf[9], double s[3], float Vf_out[9]) {
   double S[6];
   S[0] = A[0] * A[0] + A[3] * A[3] + A[6] * A[6];
@@ -1346,7 +1351,7 @@ __device__ void svd3_warm(const double A[9], float Uf[9], double s[3], float Vf_
   float a01 = (float)S[3], a02 = (float)S[4], a12 = (float)S[5];
   float Vf[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
 #pragma unroll 1
-  for (int sweep = 0; sweep < 5; ++sweep) {
+  for (int sweep = 0; sweep < PM_SVD_WARM_SWEEPS; ++sweep) {
     jrot_f32(a00, a11, a01, a02, a12, Vf, 0, 1);  // pair (0,1), third index 2
     jrot_f32(a00, a22, a02, a01, a12, Vf, 0, 2);  // pair (0,2), third index 1
     jrot_f32(a11, a22, a12, a01, a02, Vf, 1, 2);  // pair (1,2), third index 0
@@ -1403,29 +1408,51 @@ __device__ void svd3_warm(const double A[9], float Uf[9], double s[3], float Vf_
     if (!rotated) break;
   }
   // singular values in FP64; U = W diag(1/s) and V rounded to FP32 (fixed indices throughout, so
-  // the factors stay in registers)
+  // the factors stay in registers).  A column whose singular value is below 1e-6 of the largest
+  // carries no reliable direction in W / s; those columns are completed from the others instead
+  // (cross product, so that det U = det V = +1), which keeps U orthogonal for (near-)singular A.
+#pragma unroll
+  for (int j = 0; j < 3; ++j) s[j] = sqrt(W[j] * W[j] + W[3 + j] * W[3 + j] + W[6 + j] * W[6 + j]);
+  const double smax = fmax(s[0], fmax(s[1], s[2]));
   bool ok[3];
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
-    s[j] = sqrt(W[j] * W[j] + W[3 + j] * W[3 + j] + W[6 + j] * W[6 + j]);
-    ok[j] = s[j] > 1e-300;
+    ok[j] = s[j] > 1e-6 * smax && s[j] > 1e-300;
     const float inv = ok[j] ? (float)(1.0 / s[j]) : 0.f;
 #pragma unroll
     for (int k = 0; k < 3; ++k) Uf[3 * k + j] = (float)W[3 * k + j] * inv;
   }
 #pragma unroll
   for (int k = 0; k < 9; ++k) Vf_out[k] = (float)V[k];
-  const int zero_cols = (!ok[0]) + (!ok[1]) + (!ok[2]);
-  if (zero_cols == 1) {  // complete U with the cross product of its other two columns
-    auto cross_col = [&](int z, int a, int b) {
-      Uf[0 + z] = Uf[3 + a] * Uf[6 + b] - Uf[6 + a] * Uf[3 + b];
-      Uf[3 + z] = Uf[6 + a] * Uf[0 + b] - Uf[0 + a] * Uf[6 + b];
-      Uf[6 + z] = Uf[0 + a] * Uf[3 + b] - Uf[3 + a] * Uf[0 + b];
-    };
+  const int bad = (!ok[0]) + (!ok[1]) + (!ok[2]);
+  auto cross_col = [&](int z, int a, int b) {  // column z = column a x column b
+    Uf[0 + z] = Uf[3 + a] * Uf[6 + b] - Uf[6 + a] * Uf[3 + b];
+    Uf[3 + z] = Uf[6 + a] * Uf[0 + b] - Uf[0 + a] * Uf[6 + b];
+    Uf[6 + z] = Uf[0 + a] * Uf[3 + b] - Uf[3 + a] * Uf[0 + b];
+  };
+  // column z = the unit vector orthogonal to column g built from the basis axis least aligned with it
+  auto perp_col = [&](int z, int g) {
+    const float gx = Uf[g], gy = Uf[3 + g], gz = Uf[6 + g];
+    float e[3] = {0.f, 0.f, 0.f};
+    if (fabsf(gx) <= fabsf(gy) && fabsf(gx) <= fabsf(gz)) e[0] = 1.f;
+    else if (fabsf(gy) <= fabsf(gz)) e[1] = 1.f;
+    else e[2] = 1.f;
+    const float d = e[0] * gx + e[1] * gy + e[2] * gz;
+    float p[3] = {e[0] - d * gx, e[1] - d * gy, e[2] - d * gz};
+    const float nrm = rsqrtf(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+    Uf[z] = p[0] * nrm;
+    Uf[3 + z] = p[1] * nrm;
+    Uf[6 + z] = p[2] * nrm;
+  };
+  if (bad == 1) {
     if (!ok[0]) cross_col(0, 1, 2);
     else if (!ok[1]) cross_col(1, 2, 0);
     else cross_col(2, 0, 1);
-  } else if (zero_cols > 1) {
+  } else if (bad == 2) {
+    if (ok[0]) { perp_col(1, 0); cross_col(2, 0, 1); }
+    else if (ok[1]) { perp_col(2, 1); cross_col(0, 1, 2); }
+    else { perp_col(0, 2); cross_col(1, 2, 0); }
+  } else if (bad == 3) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) Uf[k] = (k % 4 == 0) ? 1.f : 0.f;
   }
@@ -2318,6 +2345,28 @@ void launch_load_fields(const Params& P, const float* in, const uint8_t* active,
   const int sms = g_num_sms > 0 ? g_num_sms : 148;
   k_load_fields<<<sms * 4, 256, 0, s>>>(P, in, active, pbuf, meta);
 }
+// Self-test of the device SVD: the step's svd3_warm on n caller matrices (row-major, FP64).
+__global__ void k_svd3_batch(const double* __restrict__ A, int n, float* __restrict__ U, double* __restrict__ S,
+                             float* __restrict__ V) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double a[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[k] = A[(size_t)i * 9 + k];
+    float u[9], v[9];
+    double sg[3];
+    svd3_warm(a, u, sg, v);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { U[(size_t)i * 9 + k] = u[k]; V[(size_t)i * 9 + k] = v[k]; }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) S[(size_t)i * 3 + k] = sg[k];
+  }
+}
+void launch_svd3_batch(const double* A, int n, float* U, double* S, float* V, cudaStream_t s) {
+  if (n <= 0) return;
+  const int blocks = std::min((n + 127) / 128, (g_num_sms > 0 ? g_num_sms : 148) * 8);
+  k_svd3_batch<<<blocks, 128, 0, s>>>(A, n, U, S, V);
+}
+
 void launch_ply_particles(const Params& P, const float* pcur, const uint32_t* meta, float* out, cudaStream_t s) {
   const int sms = g_num_sms > 0 ? g_num_sms : 148;
   k_ply_particles<<<sms * 4, 256, 0, s>>>(P, pcur, meta, out);

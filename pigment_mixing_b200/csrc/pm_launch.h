@@ -73,6 +73,8 @@ cudaError_t launch_ids_to_pid(const uint32_t* ids, const uint32_t* meta, const u
 cudaError_t launch_anisotropy(const Params& P, const float* pcur, const uint32_t* meta, const DensityGeom& g,
                               const RenderScratch& r, const AnisoParams& ap, float kern, float iso, float* G,
                               float* Ginv, float* det, float* density, cudaStream_t s);
+// The step's device SVD on n row-major FP64 matrices (self-test entry point).
+void launch_svd3_batch(const double* A, int n, float* U, double* S, float* V, cudaStream_t s);
 // Poisson-disk dart throwing into a background grid of nx*ny*nz cells of side cs (= r / sqrt(3)):
 // cells[c] = (x, y, z, 1) for a cell holding a sample, 0 otherwise.
 cudaError_t poisson_fill(float4* cells, int nx, int ny, int nz, float cs, float r, uint32_t seed, uint32_t passes,

@@ -238,3 +238,45 @@ def test_ragged_particle_counts_match_oracle(count):
     assert np.abs(pg.latent - po["latent"]).max() <= 1e-5
     assert np.abs(pg.v - po["v"]).max() <= 1e-3 * max(1.0, np.abs(po["v"]).max())
     assert g.errorFlags() == 0
+
+
+@pytest.mark.gpu
+def test_device_svd_on_hard_matrices():
+    """The step's device SVD (FP32 warm start, FP64 one-sided Jacobi) on matrices that stress
+    it: random, near-identity, repeated and clustered singular values, large condition numbers,
+    large rotations, a reflection, rank-deficient.  A = U diag(s) V^T to FP32 factor rounding,
+    s equal to numpy's singular values in FP64."""
+    import ctypes as C
+    from pigment_mixing_b200._lib import call
+    rng = np.random.default_rng(7)
+
+    def rot(rng):
+        q, r = np.linalg.qr(rng.normal(size=(3, 3)))
+        q *= np.sign(np.diag(r))
+        return q if np.linalg.det(q) > 0 else -q
+
+    mats = [rng.normal(size=(3, 3)) for _ in range(200)]
+    mats += [np.eye(3) + 1e-4 * rng.normal(size=(3, 3)) for _ in range(100)]
+    for s in ([1, 1, 1], [2, 2, 0.5], [1, 1 + 1e-9, 3], [1e4, 1, 1e-4], [5, 1e-3, 1e-3], [1, 0.5, 0.0],
+              [1, 0.0, 0.0], [0.3, 0.3, 0.3 + 1e-12]):
+        for _ in range(20):
+            mats.append(rot(rng) @ np.diag(s) @ rot(rng).T)
+    mats.append(np.diag([1.0, 1.0, -1.0]))
+    mats.append(np.zeros((3, 3)))
+    A = np.ascontiguousarray(np.array(mats, np.float64))
+    n = len(A)
+    U = np.zeros((n, 3, 3), np.float32)
+    V = np.zeros((n, 3, 3), np.float32)
+    S = np.zeros((n, 3), np.float64)
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    call("pm_svd3_batch", 0, ptr(A), n, ptr(U), ptr(S), ptr(V))
+    ref = np.linalg.svd(A, compute_uv=False)
+    scale = np.maximum(ref[:, :1], 1e-300)
+    assert np.all(S >= 0.0)
+    assert np.abs(np.sort(S, 1)[:, ::-1] - ref).max(initial=0.0) <= 1e-12 * max(1.0, ref.max())
+    rec = np.einsum("nij,nj,nkj->nik", U.astype(np.float64), S, V.astype(np.float64))
+    assert (np.abs(rec - A).max(axis=(1, 2)) / scale[:, 0]).max() <= 2e-6
+    eye = np.eye(3)
+    for Q in (U, V):
+        Qd = Q.astype(np.float64)
+        assert np.abs(np.einsum("nji,njk->nik", Qd, Qd) - eye).max() <= 2e-6
