@@ -502,6 +502,7 @@ def _batch_leg(args, device, dist, ws):
     tuning, tuned_ms = b.autotune(trial_rounds=6)
     tune_s = time.perf_counter() - t0
     b.step(args.warmup)
+    pre_steps = min(g.steps_done for g in sims)  # the sequential run is timed at the same steps
     stream = torch.cuda.ExternalStream(b.stream(), device=device)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     _barrier(dist, device)
@@ -518,10 +519,11 @@ def _batch_leg(args, device, dist, ws):
     b.close()
     for g in sims:
         g.close()
-    # the same scenes, one after another through pm_advance (each synchronises at its end)
+    # the same scenes, one after another through pm_advance (each synchronises at its end), timed
+    # over the same steps of the scenes as the batch (scenes get heavier as the knife works them)
     seq = make()
     for g in seq:
-        g.advance(args.warmup)
+        g.advance(pre_steps)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
     for g in seq:
@@ -538,6 +540,7 @@ def _batch_leg(args, device, dist, ws):
             "rounds": args.batch_steps, "ms_per_round": ms / args.batch_steps, "tuning": tuning,
             "autotune_ms_per_round": tuned_ms, "autotune_seconds": tune_s,
             "sequential_value": seq_value, "speedup_vs_sequential": value / seq_value,
+            "timed_steps": [pre_steps, pre_steps + args.batch_steps],
             "steps_after": steps, "error_flags": flags, "kernel_ms": prof,
             "workload": "palette scenes: 2 blocks each, random pigment pair of 6 RGB seeds, yield U(50,200) Pa, "
                         "random 3-segment knife path, VMVisc, MUSL, APIC, plain return map"}

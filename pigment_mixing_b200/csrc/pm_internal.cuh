@@ -226,6 +226,24 @@ __device__ __forceinline__ void batch_slot(const int* __restrict__ off, int ns, 
   nblk = off[lo + 1] - off[lo];
 }
 
+// A batched CTA's scene (its constants and this step's buffers) copied into shared memory: the
+// kernel bodies then read their parameters from shared memory instead of the scene table in
+// global memory, which also frees the registers the compiler would hoist those loads into.
+struct SceneShared {
+  Params P;
+  Bufs B;
+};
+static_assert(sizeof(Params) % 4 == 0 && sizeof(Bufs) % 4 == 0, "word copy");
+__device__ __forceinline__ void load_scene_shared(const SceneDev& d, SceneShared& ss) {
+  const int* sp = reinterpret_cast<const int*>(&d.P);
+  int* dp = reinterpret_cast<int*>(&ss.P);
+  for (int k = threadIdx.x; k < (int)(sizeof(Params) / 4); k += blockDim.x) dp[k] = sp[k];
+  const int* sb = reinterpret_cast<const int*>(&d.B[scene_parity(d)]);
+  int* db = reinterpret_cast<int*>(&ss.B);
+  for (int k = threadIdx.x; k < (int)(sizeof(Bufs) / 4); k += blockDim.x) db[k] = sb[k];
+  __syncthreads();
+}
+
 // Order-preserving float <-> int key (min/max of floats through integer atomics).
 __host__ __device__ inline int fkey(float f) {
   int i;

@@ -798,8 +798,9 @@ __global__ void __launch_bounds__(kThreads) k_p2g(Params P, Bufs B) { d_p2g(P, B
 __global__ void __launch_bounds__(kThreads) kb_p2g(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
   int s_, blk_, nblk_;
   batch_slot(off, ns, s_, blk_, nblk_);
-  const SceneDev& d_ = sd[s_];
-  d_p2g(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+  __shared__ SceneShared ss_;
+  load_scene_shared(sd[s_], ss_);
+  d_p2g(ss_.P, ss_.B, blk_, nblk_);
 }
 
 
@@ -1034,8 +1035,9 @@ __global__ void k_grid_update(Params P, Bufs B) { d_grid_update(P, B, blockIdx.x
 __global__ void kb_grid_update(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
   int s_, blk_, nblk_;
   batch_slot(off, ns, s_, blk_, nblk_);
-  const SceneDev& d_ = sd[s_];
-  d_grid_update(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+  __shared__ SceneShared ss_;
+  load_scene_shared(sd[s_], ss_);
+  d_grid_update(ss_.P, ss_.B, blk_, nblk_);
 }
 
 
@@ -1293,8 +1295,9 @@ __global__ void __launch_bounds__(kThreads, PM_G2P_MINB) kb_g2p_musl(const Scene
                                                                      const int* __restrict__ off, int ns) {
   int s_, blk_, nblk_;
   batch_slot(off, ns, s_, blk_, nblk_);
-  const SceneDev& d_ = sd[s_];
-  d_g2p_musl<kFlip>(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+  __shared__ SceneShared ss_;
+  load_scene_shared(sd[s_], ss_);
+  d_g2p_musl<kFlip>(ss_.P, ss_.B, blk_, nblk_);
 }
 
 
@@ -1958,16 +1961,18 @@ __global__ void __launch_bounds__(kThreads, PM_HEAD_MINB) kb_defgrad_head(const 
                                                                const int* __restrict__ off, int ns) {
   int s_, blk_, nblk_;
   batch_slot(off, ns, s_, blk_, nblk_);
-  const SceneDev& d_ = sd[s_];
-  d_defgrad<PL_NONE, false, 1>(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+  __shared__ SceneShared ss_;
+  load_scene_shared(sd[s_], ss_);
+  d_defgrad<PL_NONE, false, 1>(ss_.P, ss_.B, blk_, nblk_);
 }
 template <int kModel, bool kExtras>
 __global__ void __launch_bounds__(kThreads, PM_DEFGRAD_MINB) kb_defgrad_tail(const SceneDev* __restrict__ sd,
                                                                              const int* __restrict__ off, int ns) {
   int s_, blk_, nblk_;
   batch_slot(off, ns, s_, blk_, nblk_);
-  const SceneDev& d_ = sd[s_];
-  d_defgrad<kModel, kExtras, 2>(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+  __shared__ SceneShared ss_;
+  load_scene_shared(sd[s_], ss_);
+  d_defgrad<kModel, kExtras, 2>(ss_.P, ss_.B, blk_, nblk_);
 }
 
 
