@@ -442,9 +442,9 @@ pm_status pm_create(int device, pm_sim** out) {
   if (e != cudaSuccess || count == 0) return fail(PM_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
   if (device < 0 || device >= count) return fail(PM_ERR_INVALID, "device ordinal out of range");
   CK(cudaSetDevice(device));
-  cudaDeviceProp prop;
-  CK(cudaGetDeviceProperties(&prop, device));
-  if (prop.major < 10) return fail(PM_ERR_UNSUPPORTED, "this library is built for sm_100a (B200) only");
+  int major = 0;  // one attribute query (the full property query costs milliseconds)
+  CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  if (major < 10) return fail(PM_ERR_UNSUPPORTED, "this library is built for sm_100a (B200) only");
   pm_sim* s = new pm_sim();
   s->device = device;
   if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) { delete s; return fail(PM_ERR_CUDA, "stream"); }
@@ -679,18 +679,10 @@ pm_status pm_set_particles(pm_sim* sim, uint32_t n, const float* x, const float*
   sim->np = n;
   sim->np_stride = (int)((n + 31) / 32 * 32);
   const size_t S = (size_t)std::max(sim->np_stride, 32);
-  for (int k = 0; k < 2; ++k) {
-    CK(cudaMalloc(&sim->d_pbuf[k], S * F_COUNT * sizeof(float)));
-    CK(cudaMalloc(&sim->d_meta[k], S * sizeof(uint32_t)));
-  }
-  CK(cudaMalloc(&sim->d_pic, S * 6 * sizeof(float)));
-  CK(cudaMalloc(&sim->d_key, S * sizeof(uint32_t)));
-  CK(cudaMalloc(&sim->d_rank, S * sizeof(uint32_t)));
-  CK(cudaMalloc(&sim->d_sorted, S * sizeof(uint32_t)));
-  CK(cudaMalloc(&sim->d_unperm, (size_t)std::max(n, 1u) * F_COUNT * sizeof(float)));
-  CK(cudaMalloc(&sim->d_active, std::max(n, 1u)));
   // stage the host arrays on the device (d_unperm holds n*42 floats >= n*13) and scatter them
-  // into the structure-of-arrays state there
+  // into the structure-of-arrays state there; the staging buffer comes first so that the copies
+  // (asynchronous from pinned host memory) run while the other buffers are allocated
+  CK(cudaMalloc(&sim->d_unperm, (size_t)std::max(n, 1u) * F_COUNT * sizeof(float)));
   float* dx_ = sim->d_unperm;
   float* dl_ = dx_ + (size_t)n * 3;
   float* dv_ = dl_ + (size_t)n * 7;
@@ -699,6 +691,15 @@ pm_status pm_set_particles(pm_sim* sim, uint32_t n, const float* x, const float*
     if (latent) CK(cudaMemcpyAsync(dl_, latent, (size_t)n * 7 * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
     if (v) CK(cudaMemcpyAsync(dv_, v, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
   }
+  for (int k = 0; k < 2; ++k) {
+    CK(cudaMalloc(&sim->d_pbuf[k], S * F_COUNT * sizeof(float)));
+    CK(cudaMalloc(&sim->d_meta[k], S * sizeof(uint32_t)));
+  }
+  CK(cudaMalloc(&sim->d_pic, S * 6 * sizeof(float)));
+  CK(cudaMalloc(&sim->d_key, S * sizeof(uint32_t)));
+  CK(cudaMalloc(&sim->d_rank, S * sizeof(uint32_t)));
+  CK(cudaMalloc(&sim->d_sorted, S * sizeof(uint32_t)));
+  CK(cudaMalloc(&sim->d_active, std::max(n, 1u)));
   Params up{};
   up.np = (int)n;
   up.np_stride = (int)S;

@@ -21,6 +21,8 @@
 #include <algorithm>
 #include <cstdint>
 #include <cmath>
+#include <mutex>
+#include <vector>
 #include "pm_internal.cuh"
 #include "pm_launch.h"
 
@@ -2167,7 +2169,21 @@ static int g_num_sms = 0;
 static int g_occ_p2g = 1, g_occ_g2p = 1, g_occ_def = 1;
 int scan_ctas_for(int node_cap, int max_ctas);
 
+// Kernel attributes and launch shapes, set once per device (later calls return at once).
 cudaError_t launch_init(int device) {
+  static std::mutex mu;
+  static std::vector<char> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (device >= 0 && device < (int)done.size() && done[device]) return cudaSuccess;
+  cudaError_t e = launch_init_device(device);
+  if (e == cudaSuccess && device >= 0) {
+    if ((int)done.size() <= device) done.resize(device + 1, 0);
+    done[device] = 1;
+  }
+  return e;
+}
+
+cudaError_t launch_init_device(int device) {
   cudaError_t e = cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem_bytes());

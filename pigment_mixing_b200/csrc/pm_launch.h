@@ -7,7 +7,8 @@
 
 namespace pm {
 
-cudaError_t launch_init(int device);
+cudaError_t launch_init(int device);         // once per device; later calls return at once
+cudaError_t launch_init_device(int device);  // the set-up itself
 int num_sms();
 int kernels_per_step(const Params& P);
 const char* kernel_name(int i, const Params& P);
