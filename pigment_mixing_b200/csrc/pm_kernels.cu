@@ -4,7 +4,8 @@
 //   k_prologue      dt (update_dt.cpp:5-41) and the step's grid box (remesh.cpp:182-297)
 //   k_clear         zero cell counters and the main grid records
 //   k_count         per particle: cell key + rank (counting sort, pass 1)
-//   k_scan_*        exclusive prefix of the cell counters -> cell starts
+//   k_scan_local,   exclusive prefix of the cell counters -> cell starts (block scans, then the
+//   k_scan_add      block offsets, each formed by the CTA that adds it)
 //   k_scatter       counting sort, pass 2: new position -> read index
 //   k_p2g           P2G + particle half of the explicit update (p2g.cpp:6-126,
 //                   explicit_euler_update.cpp:12-55) with the cached Kirchhoff stress
@@ -494,44 +495,47 @@ __global__ void __launch_bounds__(kScanThreads) kb_scan_local(const SceneDev* __
 }
 
 
-__device__ __forceinline__ void d_scan_top(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
-  const Ctrl* c = B.ctrl;
-  if (c->halt || c->idle) return;
-  const int n = c->n_nodes + 1;
-  const int nblk = (n + kScanBlock - 1) / kScanBlock;
-  __shared__ uint32_t ws[32];
-  __shared__ uint32_t carry_s;
-  if (threadIdx.x == 0) carry_s = 0;
+// Sum of v[a, b) over the block (all threads call it; ws: 33 words of shared memory).
+__device__ __forceinline__ uint32_t block_range_sum(const uint32_t* __restrict__ v, int a, int b, uint32_t* ws) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t t = 0;
+  for (int j = a + threadIdx.x; j < b; j += blockDim.x) t += v[j];
+  t = __reduce_add_sync(0xffffffffu, t);
+  if (lane == 0) ws[wid] = t;
   __syncthreads();
-  for (int s0 = 0; s0 < nblk; s0 += kScanThreads) {
-    int i = s0 + threadIdx.x;
-    uint32_t v = i < nblk ? B.scan_part[i] : 0u;
-    uint32_t incl = block_incl_scan(v, ws);
-    uint32_t carry = carry_s;
-    if (i < nblk) B.scan_part[i] = carry + incl - v;
-    __syncthreads();
-    if (threadIdx.x == kScanThreads - 1) carry_s = carry + incl;
-    __syncthreads();
+  if (wid == 0) {
+    uint32_t u = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0u;
+    u = __reduce_add_sync(0xffffffffu, u);
+    if (lane == 0) ws[32] = u;
   }
-  if (threadIdx.x == 0) B.cell[n] = carry_s;  // total = np
-}
-__global__ void __launch_bounds__(kScanThreads) k_scan_top(Params P, Bufs B) { d_scan_top(P, B, blockIdx.x, gridDim.x); }
-__global__ void __launch_bounds__(kScanThreads) kb_scan_top(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
-  int s_, blk_, nblk_;
-  batch_slot(off, ns, s_, blk_, nblk_);
-  const SceneDev& d_ = sd[s_];
-  d_scan_top(d_.P, d_.B[scene_parity(d_)], blk_, nblk_);
+  __syncthreads();
+  const uint32_t r = ws[32];
+  __syncthreads();  // ws is reused by the next call
+  return r;
 }
 
-
+// Second scan pass: adds to every scan block the sum of the block totals before it, each CTA
+// extending its running prefix over the blocks it skipped (grid-stride), and CTA 0 writes the
+// grand total behind the last cell.  Forming the prefixes here replaces a separate one-CTA pass
+// over the block totals.
 __device__ __forceinline__ void d_scan_add(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
   if (c->halt || c->idle) return;
   const int n = c->n_nodes + 1;
-  for (int sb = blk_ > 0 ? blk_ : nblk_; sb * kScanBlock < n; sb += nblk_) {  // block 0 needs no offset
+  const int nb = (n + kScanBlock - 1) / kScanBlock;
+  __shared__ uint32_t ws[33];
+  uint32_t off = 0;  // sum of scan_part[0, upto)
+  int upto = 0;
+  for (int sb = blk_; sb < nb; sb += nblk_) {
+    off += block_range_sum(B.scan_part, upto, sb, ws);
+    upto = sb;
+    if (sb == 0) continue;  // block 0 needs no offset
     const int b0 = sb * kScanBlock;
-    const uint32_t off = B.scan_part[sb];
     for (int i = b0 + threadIdx.x; i < min(b0 + kScanBlock, n); i += kScanThreads) B.cell[i] += off;
+  }
+  if (blk_ == 0) {
+    const uint32_t total = block_range_sum(B.scan_part, 0, nb, ws);
+    if (threadIdx.x == 0) B.cell[n] = total;  // = np
   }
 }
 __global__ void __launch_bounds__(kScanThreads) k_scan_add(Params P, Bufs B) { d_scan_add(P, B, blockIdx.x, gridDim.x); }
@@ -2210,14 +2214,14 @@ cudaError_t launch_init_device(int device) {
 int num_sms() { return g_num_sms; }
 
 // The kernels of one step in launch order (the surrogate pass adds k_mlp_infer and k_sur_finish).
-static const char* kKernelNames[16] = {"k_prologue",     "k_clear",        "k_count",     "k_scan_local",
-                                       "k_scan_top",     "k_scan_add",     "k_scatter",   "k_clear_bricks",
-                                       "k_p2g",          "k_grid_update",  "k_g2p_musl",  "k_defgrad_head",
-                                       "k_defgrad_tail", "k_mlp_infer",    "k_sur_finish", "k_epilogue"};
-int kernels_per_step(const Params& P) { return P.return_map == 1 ? 16 : 14; }
+static const char* kKernelNames[15] = {"k_prologue",     "k_clear",        "k_count",     "k_scan_local",
+                                       "k_scan_add",     "k_scatter",      "k_clear_bricks", "k_p2g",
+                                       "k_grid_update",  "k_g2p_musl",     "k_defgrad_head", "k_defgrad_tail",
+                                       "k_mlp_infer",    "k_sur_finish",   "k_epilogue"};
+int kernels_per_step(const Params& P) { return P.return_map == 1 ? 15 : 13; }
 const char* kernel_name(int i, const Params& P) {
   if (i < 0 || i >= kernels_per_step(P)) return "";
-  if (P.return_map != 1 && i == 13) return kKernelNames[15];
+  if (P.return_map != 1 && i == 12) return kKernelNames[14];
   return kKernelNames[i];
 }
 
@@ -2234,7 +2238,6 @@ void launch_step(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev
   k_clear<<<flat_grid, 256, 0, s>>>(P, B); mark();
   k_count<<<flat_grid, 256, 0, s>>>(P, B); mark();
   k_scan_local<<<scan_blocks, kScanThreads, 0, s>>>(P, B); mark();
-  k_scan_top<<<1, kScanThreads, 0, s>>>(P, B); mark();
   k_scan_add<<<scan_blocks, kScanThreads, 0, s>>>(P, B); mark();
   k_scatter<<<flat_grid, 256, 0, s>>>(P, B); mark();
   k_clear_bricks<<<flat_grid, 256, 0, s>>>(P, B); mark();
@@ -2263,14 +2266,14 @@ void launch_step(const Params& P, const Bufs& B, cudaStream_t s, cudaEvent_t* ev
 // ------------------------------------------------------------------------------------------
 // batched scenes: every kernel of the step launched once for all scenes
 // ------------------------------------------------------------------------------------------
-static const char* kBatchKernelNames[16] = {
-    "kb_prologue", "kb_clear", "kb_count", "kb_scan_local", "kb_scan_top", "kb_scan_add", "kb_scatter",
-    "kb_clear_bricks", "kb_p2g", "kb_grid_update", "kb_g2p_musl", "kb_defgrad_head", "kb_defgrad_tail",
-    "kb_mlp_infer", "kb_sur_finish", "kb_epilogue"};
-int batched_kernels_per_step(bool surrogate) { return surrogate ? 16 : 14; }
+static const char* kBatchKernelNames[15] = {
+    "kb_prologue", "kb_clear", "kb_count", "kb_scan_local", "kb_scan_add", "kb_scatter", "kb_clear_bricks",
+    "kb_p2g", "kb_grid_update", "kb_g2p_musl", "kb_defgrad_head", "kb_defgrad_tail", "kb_mlp_infer",
+    "kb_sur_finish", "kb_epilogue"};
+int batched_kernels_per_step(bool surrogate) { return surrogate ? 15 : 13; }
 const char* batched_kernel_name(int i, bool surrogate) {
   if (i < 0 || i >= batched_kernels_per_step(surrogate)) return "";
-  if (!surrogate && i == 13) return kBatchKernelNames[15];
+  if (!surrogate && i == 12) return kBatchKernelNames[14];
   return kBatchKernelNames[i];
 }
 void batched_occupancy(int& p2g, int& g2p, int& def) {
@@ -2298,7 +2301,6 @@ void launch_step_batched(const BatchLaunch& L, cudaStream_t s, cudaEvent_t* ev) 
   kb_clear<<<L.n_node, ft, 0, s>>>(sd, L.off_node, ns); mark();
   kb_count<<<L.n_part, ft, 0, s>>>(sd, L.off_part, ns); mark();
   kb_scan_local<<<L.n_scan, kScanThreads, 0, s>>>(sd, L.off_scan, ns); mark();
-  kb_scan_top<<<ns, kScanThreads, 0, s>>>(sd, L.off_unit, ns); mark();
   kb_scan_add<<<L.n_scan, kScanThreads, 0, s>>>(sd, L.off_scan, ns); mark();
   kb_scatter<<<L.n_part, ft, 0, s>>>(sd, L.off_part, ns); mark();
   kb_clear_bricks<<<L.n_node, ft, 0, s>>>(sd, L.off_node, ns); mark();

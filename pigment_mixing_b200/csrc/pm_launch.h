@@ -89,7 +89,7 @@ void launch_load_fields(const Params& P, const float* in, const uint8_t* active,
 struct BatchLaunch {
   const SceneDev* sd = nullptr;
   int ns = 0;
-  const int* off_unit = nullptr;  // one CTA per scene (prologue, scan_top, epilogue)
+  const int* off_unit = nullptr;  // one CTA per scene (prologue, epilogue)
   const int* off_part = nullptr;  // particle-parallel flat kernels (count, scatter)
   const int* off_node = nullptr;  // node-parallel flat kernels (clear, clear_bricks, grid_update)
   const int* off_scan = nullptr;  // scan blocks of each scene's cell array
