@@ -361,7 +361,12 @@ def run_ours(args):
         batch = _batch_leg(args, device, dist, ws)
     # -------- end to end through the C ABI from pinned host buffers --------
     _e2e(scene, args, device, dist, ws)  # untimed pass: first-use costs of the API path (allocator, streams)
-    e2e = _e2e(scene, args, device, dist, ws)
+    # three timed passes, the median reported: one pass is about a tenth of a second of host and
+    # device work, so the host's own noise (page faults, other tenants) moves single passes
+    runs = sorted((_e2e(scene, args, device, dist, ws) for _ in range(3)), key=lambda r: r["value"])
+    e2e = dict(runs[1])
+    e2e["passes"] = [r["value"] for r in runs]
+    e2e["includes"] += "; median of three timed passes"
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": _config(scene, args),

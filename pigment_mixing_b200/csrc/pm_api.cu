@@ -11,6 +11,7 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <sstream>
 #include <string>
@@ -91,6 +92,32 @@ bool parse_flat_json(const std::string& text, std::map<std::string, double>& out
   return false;
 }
 
+}  // namespace
+
+// Pinned host mirrors of the control blocks come from a process-wide pool: a page-locked
+// allocation costs about a millisecond, a free slot of the pool nothing.  The pool grows by slabs
+// of 16 portable pinned blocks, kept until the process exits.
+namespace {
+std::mutex g_ctrl_mu;
+std::vector<Ctrl*> g_ctrl_free;
+Ctrl* ctrl_mirror_get() {
+  std::lock_guard<std::mutex> lock(g_ctrl_mu);
+  if (g_ctrl_free.empty()) {
+    void* slab = nullptr;
+    if (cudaHostAlloc(&slab, 16 * sizeof(Ctrl), cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    for (int k = 15; k >= 0; --k) g_ctrl_free.push_back(static_cast<Ctrl*>(slab) + k);
+  }
+  Ctrl* c = g_ctrl_free.back();
+  g_ctrl_free.pop_back();
+  return c;
+}
+void ctrl_mirror_put(Ctrl* c) {
+  std::lock_guard<std::mutex> lock(g_ctrl_mu);
+  g_ctrl_free.push_back(c);
+}
 }  // namespace
 
 struct pm_sim {
@@ -186,10 +213,9 @@ pm_sim::~pm_sim() {
   drop_graphs();
   free_particles();
   free_grid();
-  if (d_ctrl) cudaFree(d_ctrl);
-  if (h_ctrl) cudaFreeHost(h_ctrl);
+  if (d_ctrl) cudaFree(d_ctrl);  // also holds d_stats
+  if (h_ctrl) ctrl_mirror_put(h_ctrl);
   if (d_frames) cudaFree(d_frames);
-  if (d_stats) cudaFree(d_stats);
   if (d_mlp) cudaFree(d_mlp);
   if (d_slog) cudaFree(d_slog);
   if (d_splat) cudaFree(d_splat);
@@ -448,11 +474,14 @@ pm_status pm_create(int device, pm_sim** out) {
   pm_sim* s = new pm_sim();
   s->device = device;
   if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) { delete s; return fail(PM_ERR_CUDA, "stream"); }
-  if (cudaMalloc(&s->d_ctrl, sizeof(Ctrl)) != cudaSuccess || cudaMallocHost(&s->h_ctrl, sizeof(Ctrl)) != cudaSuccess ||
-      cudaMalloc(&s->d_stats, 16 * sizeof(double)) != cudaSuccess) {
+  // the control block and the statistics accumulators share one device allocation
+  const size_t ctrl_bytes = (sizeof(Ctrl) + 255) / 256 * 256;
+  if (cudaMalloc(&s->d_ctrl, ctrl_bytes + 16 * sizeof(double)) != cudaSuccess ||
+      (s->h_ctrl = ctrl_mirror_get()) == nullptr) {
     delete s;
     return fail(PM_ERR_CUDA, "allocation of the control block failed");
   }
+  s->d_stats = reinterpret_cast<double*>(reinterpret_cast<char*>(s->d_ctrl) + ctrl_bytes);
   std::memset(s->h_ctrl, 0, sizeof(Ctrl));
   s->h_ctrl->knife = -1;
   e = launch_init(device);
