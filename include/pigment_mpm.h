@@ -147,6 +147,14 @@ PM_API pm_status pm_step(pm_sim* sim);
  * 270-285) -- on the device without host round trips (CUDA graph replay).  *frames_done, if not
  * NULL, receives the number of frame boundaries crossed. */
 PM_API pm_status pm_advance(pm_sim* sim, uint32_t nsteps, uint32_t* frames_done);
+/* Simulation::simulate() (simulation.cpp:86-222), the reference's offline driver used by its tests:
+ * prepares the scene (material constants, the initial grid, time = frame = 0) and steps until
+ * end_frame frames are done, with simulate()'s frame test after every step, on the device (the
+ * steps issued after the last frame idle).  The update is USL unless use_musl was set to 1 (the
+ * field's own default, simulation.hpp:49; pm_prepare turns MUSL on as prepareSimulation does).
+ * max_steps > 0 bounds the run (PM_ERR_STATE when end_frame was not reached); *steps_done, if not
+ * NULL, receives the steps taken. */
+PM_API pm_status pm_simulate(pm_sim* sim, uint32_t max_steps, uint32_t* steps_done);
 /* Simulation::frameFinished() (simulation_units.cpp:235-241): mutates `frame`. */
 PM_API pm_status pm_frame_finished(pm_sim* sim, int* finished);
 /* Simulation::isFinished() (simulation_units.cpp:243-245). */
@@ -346,20 +354,23 @@ PM_API const char* pm_batch_kernel_name(pm_batch* batch, int index);
 PM_API pm_status pm_batch_profile(pm_batch* batch, uint32_t rounds, float* kernel_ms, uint32_t n_kernels);
 
 /* ---- particle-to-grid transfer that allocates nothing --------------------------------------
- * No counterpart in the reference.  For callers that cannot call cudaMalloc: code running while
- * a CUDA graph is captured, and plug-ins whose host application owns every device allocation.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc: plug-ins whose host
+ * application owns every device allocation (a caching allocator or a fixed memory budget), loops
+ * that may not allocate once running, callers holding only raw device arrays.
  * It scatters caller-owned particle arrays onto a caller-described node box with the step's
  * P2G transfer (quadratic B-splines, counting sort by cell, one warp per cell) and the
  * reference's normalisation (p2g.cpp:97-124).  Inputs and outputs are device pointers:
  * x[n*3], v[n*3], B[n*9] (APIC matrix, NULL = none), latent[n*7], diffusion[n]; node (i,j,k) sits
  * at origin + (i,j,k)*dx and is entry (i*dims[1] + j)*dims[2] + k of node_mass[nodes],
  * node_velocity[nodes*3], node_latent[nodes*7], node_shear[nodes] (any output may be NULL).
+ * All n particles are treated as active (no active mask, unlike p2g.cpp:22).
  * Scratch is one fixed 8 MiB __device__ array inside the library (held by every GPU that loads
  * it until exit): at most 131072 particles and 131072 nodes per call, PM_ERR_CAPACITY beyond.
  * The first call on a device looks up that array's device address, so make it before any stream
  * capture.  All calls share the array: calls whose work overlaps on the GPU race.  Work is queued
- * on `stream` (NULL = default stream); when `outside` is not NULL the call waits for the stream
- * and stores the number of particles whose stencil left the box (they are skipped). */
+ * on `stream` (NULL = default stream).  When `outside` is not NULL the call synchronises `stream`
+ * and stores the number of particles skipped because their stencil left the box or a coordinate
+ * was not finite; the stream must then not be in capture mode. */
 PM_API pm_status pm_p2g_noalloc(const float* x, const float* v, const float* B, const float* latent,
                                 const float* diffusion, uint32_t n, double particle_mass, double dx,
                                 const double origin[3], const int32_t dims[3], float* node_mass,

@@ -424,6 +424,9 @@ template <class R> struct Sim {
   // public parameters (simulation.hpp:38-126)
   unsigned n_threads = 1, end_frame = 10, frame = 0;
   bool use_musl = false, use_particle_boundaries = false, use_pradhana = true;
+  // use_musl as the caller set it: prepare() turns MUSL on like prepareSimulation
+  // (simulation_units.cpp:185-186); simulate() keeps the field (false by default, simulation.hpp:49)
+  bool use_musl_user = false;
   V3<R> grid_reference_point = V3<R>(R(2e10), R(2e10), R(2e10));
   V3<R> gravity;
   V3<R> particle_boundary_min = V3<R>(-5, -5, -5), particle_boundary_max = V3<R>(5, 5, 5);
@@ -1135,7 +1138,8 @@ template <class Fn> static auto dispatch(pmo_sim* h, Fn fn) {
 template <class R> static int setParam(Sim<R>& s, const char* n, double v) {
   std::string k(n);
 #define P(name, field) if (k == name) { s.field = (decltype(s.field))v; return 0; }
-  P("n_threads", n_threads) P("end_frame", end_frame) P("frame", frame) P("use_musl", use_musl)
+  P("n_threads", n_threads) P("end_frame", end_frame) P("frame", frame)
+  if (k == "use_musl") { s.use_musl = s.use_musl_user = v != 0; return 0; }
   P("use_particle_boundaries", use_particle_boundaries) P("use_pradhana", use_pradhana) P("min_dt", min_dt)
   P("fps", fps) P("cfl", cfl) P("cfl_elastic", cfl_elastic) P("flip_ratio", flip_ratio) P("rho", rho) P("E", E)
   P("nu", nu) P("xi", xi) P("q_max", q_max) P("q_min", q_min) P("p_min", p_min) P("M", M)
@@ -1279,12 +1283,12 @@ int pmo_advance(pmo_sim* h, unsigned nsteps, unsigned* frames_done) {
   });
 }
 // The reference's offline driver: simulation.cpp:339-474 (simulate) after prepare-style setup,
-// run until end_frame, USL by default.
+// run until end_frame, USL unless use_musl was set.
 int pmo_simulate(pmo_sim* h) {
   return dispatch(h, [&](auto& s) {
     using R = std::decay_t<decltype(s.dx)>;
     s.prepare();
-    s.use_musl = false;
+    s.use_musl = s.use_musl_user;
     while (s.frame < s.end_frame) {
       s.advanceStep();
       s.time += s.dt;

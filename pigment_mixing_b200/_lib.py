@@ -42,6 +42,7 @@ SIGNATURES = {
     "pm_prepare": [_vp],
     "pm_step": [_vp],
     "pm_advance": [_vp, C.c_uint32, _up],
+    "pm_simulate": [_vp, C.c_uint32, _up],
     "pm_frame_finished": [_vp, C.POINTER(C.c_int)],
     "pm_is_finished": [_vp, C.POINTER(C.c_int)],
     "pm_get_grid_boundaries": [_vp, _dp, _dp],

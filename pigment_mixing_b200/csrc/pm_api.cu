@@ -49,6 +49,9 @@ struct HostParams {
   double end_frame = 10;
   int plastic_model = PM_NO_PLASTICITY;
   int use_pradhana = 1, use_musl = 0, use_particle_boundaries = 0, auto_frame = 0;
+  // use_musl as the caller last set it: prepareSimulation turns MUSL on (simulation_units.cpp:
+  // 185-186), simulate() keeps the field's own value (false by default, simulation.hpp:49)
+  int use_musl_user = 0;
   double gravity[3] = {0, 0, 0};
   double pbmin[3] = {-5, -5, -5}, pbmax[3] = {5, 5, 5};
   double grid_ref[3] = {2e10, 2e10, 2e10};
@@ -427,6 +430,8 @@ pm_status pm_sim::run_steps(uint32_t n, bool use_graph) {
     cur = (cur + (int)done) & 1;
     remaining -= std::min(done, remaining);
     if (done > 0) guard = 0;  // count only regrowths that made no progress
+    // a simulate() run ends with its last frame; the steps launched after it idled
+    if (h_ctrl->stop_at_end && h_ctrl->frame >= h_ctrl->end_frame && !h_ctrl->halt) return PM_OK;
     if (done == 0 && !h_ctrl->halt)
       return fail(PM_ERR_STATE, "steps made no progress (the control block holds a batch target)");
     long long want = 0;
@@ -536,7 +541,7 @@ pm_status pm_set_param(pm_sim* sim, const char* name, double v) {
   else if (k == "end_boost_time") h.end_boost = v;
   else if (k == "boost_factor") h.boost_factor = v;
   else if (k == "use_pradhana") h.use_pradhana = v != 0;
-  else if (k == "use_musl") h.use_musl = v != 0;
+  else if (k == "use_musl") h.use_musl = h.use_musl_user = v != 0;
   else if (k == "use_particle_boundaries") h.use_particle_boundaries = v != 0;
   else if (k == "plastic_model") {
     int m = (int)v;
@@ -1091,6 +1096,31 @@ pm_status pm_advance(pm_sim* sim, uint32_t nsteps, uint32_t* frames_done) {
   if (!af) { sim->h_ctrl->auto_frame = 0; pm_status s2 = sim->push_ctrl(); if (s == PM_OK) s = s2; }
   if (frames_done) *frames_done = sim->h_ctrl->frames_done - fd0;
   return s;
+}
+
+pm_status pm_simulate(pm_sim* sim, uint32_t max_steps, uint32_t* steps_done) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (steps_done) *steps_done = 0;
+  const int musl = sim->hp.use_musl_user;
+  pm_status s = pm_prepare(sim);  // material constants, the initial grid, time = frame = 0
+  if (s != PM_OK) return s;
+  sim->hp.use_musl = musl;
+  sim->fill_params();
+  Ctrl* c = sim->h_ctrl;
+  const uint32_t step0 = c->step, af = c->auto_frame;
+  c->auto_frame = 1;  // the loop's frame test after every step (simulation.cpp:184-193)
+  c->stop_at_end = 1;
+  if ((s = sim->push_ctrl()) != PM_OK) return s;
+  s = sim->run_steps(max_steps ? max_steps : 0xffffffffu, true);
+  pm_status s2 = sim->sync_ctrl();
+  c->auto_frame = af;
+  c->stop_at_end = 0;
+  if (s2 == PM_OK) s2 = sim->push_ctrl();
+  if (steps_done) *steps_done = c->step - step0;
+  if (s != PM_OK) return s;
+  if (s2 != PM_OK) return s2;
+  if (c->frame < c->end_frame) return fail(PM_ERR_STATE, "simulate: max_steps reached before end_frame");
+  return PM_OK;
 }
 
 pm_status pm_frame_finished(pm_sim* sim, int* finished) {

@@ -167,7 +167,7 @@ struct Ctrl {
   uint32_t slog_n;         // samples written to the log (cumulative)
   uint32_t target_step;    // batches: the scene idles once step reaches this (0 = no target)
   uint32_t idle;           // set by the prologue: this round is skipped for the scene
-  uint32_t pad0;
+  uint32_t stop_at_end;    // 1: steps idle once frame >= end_frame (the simulate() driver)
   // objects
   int n_plates, n_objects, knife;  // knife: index into objects or -1
   int pad1;

@@ -119,8 +119,10 @@ __device__ __forceinline__ void d_prologue(const Params& P, const Bufs& B, const
   if (threadIdx.x != 0 || blk_ != 0) return;
   Ctrl* c = B.ctrl;
   if (c->halt) return;
-  // a scene of a batch that has reached its target step sits this round out
-  c->idle = (c->target_step != 0u && c->step >= c->target_step) ? 1u : 0u;
+  // a scene of a batch that has reached its target step sits this round out, and so does a
+  // simulate() run whose last frame is done (simulation.cpp:170-203 leaves its loop there)
+  c->idle = ((c->target_step != 0u && c->step >= c->target_step) || (c->stop_at_end && c->frame >= c->end_frame))
+                ? 1u : 0u;
   if (c->idle) return;
   // updateDt (update_dt.cpp:5-41)
   float m2f = __uint_as_float(c->max_v2);

@@ -1,9 +1,9 @@
 // pm_p2g_noalloc: a particle-to-grid transfer that allocates no memory.
 //
-// Who needs it: callers that cannot call cudaMalloc -- code that runs while a CUDA graph is
-// being captured (allocation is not a capturable operation), real-time loops and plugins whose
-// host application owns every device allocation (a caching allocator or a fixed memory budget),
-// and callers that have no pm_sim at all and only hold particle arrays in device memory.
+// Who needs it: callers that cannot call cudaMalloc -- plug-ins whose host application owns every
+// device allocation (a caching allocator or a fixed memory budget that a cudaMalloc behind its
+// back would break), real-time loops that may not allocate once running, and callers that have no
+// pm_sim at all and only hold particle arrays in device memory.
 //
 // It is the transfer half of the step's P2G kernel (counting sort of particles by cell, then one
 // warp per cell accumulating its particles into the cell's 27 stencil nodes) on caller-owned
@@ -12,7 +12,9 @@
 // loads the library holds those 8 MiB until the process exits.
 //
 // Limits: at most kNaMaxParticles particles and kNaMaxNodes grid nodes per call; larger inputs
-// are rejected with PM_ERR_CAPACITY before any work is queued.
+// are rejected with PM_ERR_CAPACITY before any work is queued.  Every particle is scattered (there
+// is no active mask, unlike p2g.cpp:22); particles whose stencil leaves the box, and particles with
+// a non-finite coordinate, are skipped and counted.
 //
 // Shared state: every call uses the same array and leaves its contents behind; each call clears
 // what must start at zero before using it.  Calls whose work overlaps on the GPU (issued on
@@ -55,8 +57,9 @@ struct NaBox {
   float apicD;
 };
 
-__device__ __forceinline__ int na_cell(float x, float o, float inv_dx) {
-  return (int)floorf(__fsub_rn(__fmul_rn(__fsub_rn(x, o), inv_dx), 0.5f));
+// Position of x in units of dx relative to the stencil base: the base node is floor of it.
+__device__ __forceinline__ float na_u(float x, float o, float inv_dx) {
+  return __fsub_rn(__fmul_rn(__fsub_rn(x, o), inv_dx), 0.5f);
 }
 __device__ __forceinline__ float na_node(int g, float o, float dx) { return __fadd_rn(o, __fmul_rn((float)g, dx)); }
 __device__ __forceinline__ float na_N(float u) {
@@ -87,11 +90,16 @@ __global__ void k_na_count(NaBox b, const float* x, unsigned char* s) {
   uint32_t* err = reinterpret_cast<uint32_t*>(s + kOffErr);
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < b.n; p += stride) {
-    int c[3];
+    // the box test runs on the float coordinate, before any conversion to int: a NaN fails
+    // every comparison and an infinite or huge coordinate fails the upper bound, so no integer
+    // overflow can turn an outside particle into an in-box key
+    int c[3] = {0, 0, 0};
     bool in = true;
     for (int d = 0; d < 3; ++d) {
-      c[d] = na_cell(x[3 * p + d], b.origin[d], b.inv_dx);
-      in = in && c[d] >= 0 && c[d] + 2 < b.dims[d];
+      const float u = na_u(x[3 * p + d], b.origin[d], b.inv_dx);
+      const bool ok = u >= 0.f && u < (float)(b.dims[d] - 2);  // floor(u) in [0, dims - 3]
+      if (ok) c[d] = (int)floorf(u);
+      in = in && ok;
     }
     uint32_t k = in ? (uint32_t)((c[0] * b.dims[1] + c[1]) * b.dims[2] + c[2]) : b.nodes;
     if (!in) atomicAdd(err, 1u);

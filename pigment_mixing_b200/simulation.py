@@ -145,6 +145,13 @@ class Simulation:
         call("pm_advance", self._h, int(nsteps), C.byref(fd))
         return fd.value
 
+    def simulate(self, max_steps: int = 0) -> int:  # simulation.cpp:86-222
+        """The reference's offline driver: prepare, then step until end_frame frames are done
+        (USL unless use_musl was set to 1).  max_steps > 0 bounds the run.  Returns the steps taken."""
+        n = C.c_uint32()
+        call("pm_simulate", self._h, int(max_steps), C.byref(n))
+        return n.value
+
     def frameFinished(self) -> bool:  # simulation_units.cpp:235-241
         o = C.c_int()
         call("pm_frame_finished", self._h, C.byref(o))

@@ -70,9 +70,16 @@ def test_one_step_particles_and_grid(small_scene):
         assert err <= tol * max(1.0, scale), (kg, err)
 
 
+def _mixing_fired(latent0, latent, thresh=1e-3):
+    """Particles whose latent moved by more than thresh from its initial value (g2p.cpp:103-126)."""
+    return int((np.abs(latent.astype(np.float64) - latent0).max(1) > thresh).sum())
+
+
 def test_config1_fifty_steps_within_tolerance():
-    """32,768-particle scene (dx = 1/64): 50 steps, position error <= 1e-3 of the domain size and
-    latent error <= 1e-3 against the FP64 oracle; mass and momentum agree."""
+    """32,768-particle scene (dx = 1/64): 50 steps against the FP64 oracle.  The workload's bar is
+    1e-3 of the domain for positions and 1e-3 for latents; the observed errors are 6.3e-7 and 7e-6,
+    so the test holds them to 1e-5 and 1e-4 (a regression of more than about 15x fails).  The knife
+    has started mixing: some latents moved by more than 1e-3, identically in both."""
     from pigment_mixing_b200 import scenes
     sc = scenes.config1(seed=0)
     g, o = _pair(sc)
@@ -83,8 +90,13 @@ def test_config1_fifty_steps_within_tolerance():
     po = o.particles_f64()
     dxp = np.linalg.norm(pg.x.astype(np.float64) - po["x"], axis=1)
     dl = np.abs(pg.latent.astype(np.float64) - po["latent"]).max(1)
-    assert dxp.max() <= 1e-3, dxp.max()
-    assert dl.max() <= 1e-3, dl.max()
+    print(f"config1 50 steps: max |dx| {dxp.max():.3e}, max |dlatent| {dl.max():.3e}, "
+          f"mixed {_mixing_fired(sc['latent'], pg.latent)} (oracle {_mixing_fired(sc['latent'], po['latent'])})")
+    assert dxp.max() <= 1e-5, dxp.max()
+    assert dl.max() <= 1e-4, dl.max()
+    mixed = _mixing_fired(sc["latent"], po["latent"])
+    assert mixed > 0
+    assert abs(_mixing_fired(sc["latent"], pg.latent) - mixed) <= max(2, mixed // 100)
     st = g.stats()
     mp = sc["params"]["particle_mass"]
     assert st["mass"] == pytest.approx(mp * n, rel=1e-12)
@@ -112,8 +124,51 @@ def test_paint_default_scene_with_reference_spatula():
     po = o.particles_f64()
     assert np.abs(pg.x.astype(np.float64) - po["x"]).max() <= 1e-4
     assert np.abs(pg.latent.astype(np.float64) - po["latent"]).max() <= 1e-4
+    print(f"paint scene: mixed {_mixing_fired(sc['latent'], pg.latent)} of {n}")
     kg, ko = g.getSpatulaObject(), o.knife()
     assert np.allclose(kg[0], ko[0], atol=1e-5)
+
+
+def test_noslip_colliders_and_moving_plates_match_oracle():
+    """NoSlip on a general object (boundary_collision.cpp:36-38) and on plates, plates moving with
+    the first-frame slow-down of vmin_factor / load_factor (object_plate.hpp:136-162): a block
+    squeezed by a descending top plate and pushed by a left wall, on a NoSlip ground object."""
+    import sys
+    sys.path.insert(0, GOLDEN.rsplit("/", 1)[0])
+    import reference_kats as K
+    from oracle.oracle import OracleSim
+    from pigment_mixing_b200 import Simulation, scenes
+    base = scenes.two_block_scene(1.0 / 32, (4, 4, 4), seed=4, steps=10, knife=False, material="vmvisc")
+    dx = base["params"]["dx"]
+    x = base["x"].astype(np.float64)
+    top = float(x[:, 1].max()) + 0.5 * dx
+    left = float(x[:, 0].min()) - 0.5 * dx
+    params = dict(base["params"], fps=20.0, end_frame=1000)
+    params.pop("use_particle_boundaries")
+    sc = dict(name="squeeze", x=x, v=None, params=params, vectors=dict(gravity=[0.0, -9.81, 0.0]),
+              objects=[("ground", dict(bc=K.BC_NOSLIP, friction=0.0, y0=0.0)),
+                       ("plate", dict(pos=top, plate_type=K.PLATE_TOP, bc=K.BC_NOSLIP, friction=0.0, vy=-0.3,
+                                      vmin_factor=4.0, load_factor=1.0)),
+                       ("plate", dict(pos=left, plate_type=K.PLATE_LEFT, bc=K.BC_SLIPSTICK, friction=0.4, vx=0.2,
+                                      vmin_factor=2.0, load_factor=2.0))])
+    g = Simulation(0)
+    K.apply(sc, g)
+    g.prepareSimulation()
+    o = OracleSim(64)
+    o.set(n_threads=8)
+    K.apply(sc, o)
+    o.prepare()
+    for _ in range(4):
+        g.advance(10)
+        o.advance(10)
+    assert g.frame == o.get("frame") and g.frame >= 1  # the slow first frames are over
+    pg = g.getParticles(fields=("x", "v", "active"))
+    po = o.particles_f64()
+    assert np.abs(pg.x - po["x"]).max() <= 1e-5
+    assert np.abs(pg.v - po["v"]).max() <= 1e-4 * max(1.0, np.abs(po["v"]).max())
+    # the plates did squeeze and push the block
+    assert po["x"][:, 1].max() < top - 0.5 * dx - 1e-3
+    assert po["x"][:, 0].min() > left + 0.5 * dx + 1e-4
 
 
 def test_usl_mode_matches_oracle(small_scene):
