@@ -57,6 +57,8 @@ def _workload(name: str):
         return scenes.config1(seed=0)
     if name == "32m":
         return scenes.config5(seed=0)
+    if name == "262k":  # the same scene at dx = 1/128: the small case for profiler captures
+        return scenes.two_block_scene(1.0 / 128, (32, 32, 16), seed=0, steps=1000)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -670,13 +672,42 @@ def _e2e(scene, args, device, dist, ws):
                         "with the following steps), final readback; after one untimed pass"}
 
 
+def profile_run(args):
+    """A fixed step sequence for profiler captures: `--warm` steps through advance() (graphs),
+    `--profile` steps timed kernel by kernel with CUDA events (printed as JSON), then `--plain`
+    ordinary step() calls, which an external profiler captures launch by launch."""
+    from pigment_mixing_b200 import Simulation, scenes
+    sc = _workload(args.workload)
+    for kv in args.set:
+        k, v = kv.split("=", 1)
+        sc["params"][k] = float(v)
+    sim = Simulation(0)
+    scenes.apply(sc, sim)
+    sim.prepareSimulation()
+    sim.advance(args.warm)
+    out = {"workload": args.workload, "particles": len(sc["x"])}
+    if args.profile > 0:
+        out["kernel_ms"] = sim.profileSteps(args.profile)
+    for _ in range(args.plain):
+        sim.step()
+    out.update(plastic_count=sim.plastic_count, grid_nodes=sim.grid_nodes, error_flags=sim.errorFlags())
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="2m", choices=["2m", "8m", "32k", "32m"])
+    ap.add_argument("--workload", default="2m", choices=["2m", "8m", "32k", "32m", "262k"])
+    ap.add_argument("--profile-run", action="store_true",
+                    help="no bench line: run the profiler-capture sequence (--warm, --profile, --plain)")
+    ap.add_argument("--warm", type=int, default=10, help="profile run: steps through advance() first")
+    ap.add_argument("--profile", type=int, default=3, help="profile run: event-timed steps")
+    ap.add_argument("--plain", type=int, default=3, help="profile run: plain step() calls at the end")
+    ap.add_argument("--set", action="append", default=[], metavar="NAME=VALUE",
+                    help="profile run: override a scene parameter, e.g. --set perzyna_exp=1")
     ap.add_argument("--return-map", default="plain", choices=["plain"],
                     help="return map of the headline value (the surrogate form is reported beside it)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -690,6 +721,8 @@ def main():
     ap.add_argument("--drift-steps", type=int, default=1000,
                     help="steps of the mass / mean-latent drift run on the workload (0 = skip)")
     args = ap.parse_args()
+    if args.profile_run:
+        return profile_run(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

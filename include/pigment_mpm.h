@@ -138,6 +138,18 @@ PM_API pm_status pm_add_curve(pm_sim* sim, int bc, double friction);
  * anim_path (NULL = none), DPVisc with Pradhana correction and q_prefac = 1/sqrt(2). */
 PM_API pm_status pm_setup_scene(pm_sim* sim, float fps, const char* pigment_config_path, const char* sim_config_path,
                          const char* anim_path);
+/* Simulation::setupScene(fps, colorRatios, pigments, anim_path) (simulation_units.cpp:28-131) in the
+ * reference's own shape, with its blob scene (Simulation::blobs, simulation_blobs.cpp:7-150): one
+ * paint blob per colour ratio, k blobs, latents[k*7] the Mixbox latent of each colour.  A ratio
+ * clamped to [0.1, 0.9] sets the blob's volume on the reference's blob ladder (0.0056-0.053); the
+ * blobs are packed touching as the reference packs them, centred on the origin, and filled by
+ * Poisson-disk sampling (radius 0.01, 30 attempts, seed 42 + blob index) with dx = cbrt(27 x box
+ * volume / box samples) and particle volume dx^3 / 27 (sampleParticlesFromVdb).  The blob shape is
+ * analytic (the upper half of the superellipsoid |x/R|^2.5 + |y/H|^2.5 + |z/R|^2.5 <= 1, H = 0.55 R)
+ * instead of the reference's OpenVDB level sets.  Then everything pm_setup_scene does. */
+PM_API pm_status pm_setup_scene_blobs(pm_sim* sim, float fps, const float* color_ratios, const float* latents, uint32_t k,
+                                      const char* pigment_config_path, const char* sim_config_path,
+                                      const char* anim_path);
 /* Simulation::prepareSimulation() (simulation_units.cpp:133-215): material constants, MUSL on,
  * the initial grid (remeshFixedInit(2,2,2)), time = frame = 0.  Uploads objects. */
 PM_API pm_status pm_prepare(pm_sim* sim);

@@ -19,9 +19,11 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIBS = {}
 
 
-def build() -> None:
-    """Compile the oracle libraries (and oracle/_ref when the reference tree is present)."""
-    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+def build(reference_root: str | None = None) -> None:
+    """Compile the oracle libraries, and oracle/_ref from the reference tree at reference_root
+    (default: the environment variable PM_REFERENCE_ROOT) when that tree is present."""
+    ref = reference_root if reference_root is not None else os.environ.get("PM_REFERENCE_ROOT", "")
+    subprocess.run(["make", "-s", "-C", _HERE, f"REF={ref}"], check=True)
 
 
 def _lib(fast: bool = False) -> C.CDLL:

@@ -39,6 +39,7 @@ SIGNATURES = {
     "pm_add_ground": [_vp, C.c_int, C.c_double, C.c_double],
     "pm_add_curve": [_vp, C.c_int, C.c_double],
     "pm_setup_scene": [_vp, C.c_float, C.c_char_p, C.c_char_p, C.c_char_p],
+    "pm_setup_scene_blobs": [_vp, C.c_float, _fp, _fp, C.c_uint32, C.c_char_p, C.c_char_p, C.c_char_p],
     "pm_prepare": [_vp],
     "pm_step": [_vp],
     "pm_advance": [_vp, C.c_uint32, _up],

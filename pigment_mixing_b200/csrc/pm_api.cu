@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cctype>
 #include <chrono>
 #include <cmath>
@@ -939,10 +940,9 @@ pm_status pm_add_curve(pm_sim* sim, int bc, double friction) {
   return PM_OK;
 }
 
-pm_status pm_setup_scene(pm_sim* sim, float fps, const char* pigment_config_path, const char* sim_config_path,
-                         const char* anim_path) {
-  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
-  if (sim->np == 0) return fail(PM_ERR_STATE, "pm_setup_scene needs particles: call pm_set_particles first");
+// Everything of setupScene after the particles exist (simulation_units.cpp:31-131 without blobs()).
+static pm_status setup_scene_common(pm_sim* sim, float fps, const char* pigment_config_path,
+                                    const char* sim_config_path, const char* anim_path) {
   pm_status s;
   if (pigment_config_path && (s = pm_load_pigment_config(sim, pigment_config_path)) != PM_OK) return s;
   if (sim_config_path && (s = pm_load_sim_config(sim, sim_config_path)) != PM_OK) return s;
@@ -957,6 +957,126 @@ pm_status pm_setup_scene(pm_sim* sim, float fps, const char* pigment_config_path
   h.plastic_model = PM_DPVISC;
   h.use_pradhana = 1;
   h.q_prefac = 1.0 / std::sqrt(2.0);
+  return PM_OK;
+}
+
+pm_status pm_setup_scene(pm_sim* sim, float fps, const char* pigment_config_path, const char* sim_config_path,
+                         const char* anim_path) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (sim->np == 0) return fail(PM_ERR_STATE, "pm_setup_scene needs particles: call pm_set_particles first");
+  return setup_scene_common(sim, fps, pigment_config_path, sim_config_path, anim_path);
+}
+
+// ---- Simulation::blobs (simulation_blobs.cpp:7-150) with analytic blobs -----------------------
+// The reference morphs pairs of OpenVDB blob level sets to each colour's target volume and samples
+// them with sampleParticlesFromVdb; here each blob is the upper half of a superellipsoid
+// |dx/R|^p + |y/H|^p + |dz/R|^p <= 1 (p = 2.5, H = 0.55 R) of exactly the target volume, packed by
+// the reference's touching arrangements and filled by Poisson-disk sampling of its bounding box.
+namespace {
+// Volumes of the reference's blob ladder (simulation.hpp:272-279, Blob_01 ... Blob_06).
+constexpr double kBlobVolumes[6] = {0.0056, 0.0151, 0.0246, 0.0341, 0.0436, 0.053};
+constexpr double kBlobAspect = 0.55, kBlobExp = 2.5;
+
+// Colour ratio -> volume: the ratio clamped to [0.1, 0.9] mapped linearly onto the ladder's
+// volume range (simulation_blobs.cpp:11-24).
+double blob_volume(double ratio) {
+  const double lo = kBlobVolumes[0], hi = kBlobVolumes[5];
+  const double r = std::min(0.9, std::max(0.1, ratio));
+  return std::min(hi, std::max(lo, lo + (r - 0.1) / 0.8 * (hi - lo)));
+}
+
+// Ground-plane offsets of touching blobs of packing radii r (simulation_blobs.cpp:63-116), centred
+// on the x / z bounds of the arrangement with y = 0 (:118-140).
+std::vector<std::array<double, 3>> blob_offsets(const std::vector<double>& r) {
+  const size_t n = r.size();
+  std::vector<std::array<double, 3>> o(n, std::array<double, 3>{0.0, 0.0, 0.0});
+  auto cz = [](double d, double dist) { return std::sqrt(std::max(0.0, dist * dist - d * d)); };
+  if (n == 2) {
+    o[0][0] = -r[0]; o[1][0] = r[1];
+  } else if (n == 3) {
+    o[1][0] = r[0] + r[1];
+    const double x1 = o[1][0];
+    const double x2 = ((r[0] + r[2]) * (r[0] + r[2]) - (r[1] + r[2]) * (r[1] + r[2]) + x1 * x1) / (2.0 * x1);
+    o[2][0] = x2;
+    o[2][2] = cz(x2, r[0] + r[2]);
+  } else if (n == 4) {
+    o[0][0] = -r[0]; o[1][0] = r[1]; o[2][0] = -r[2]; o[3][0] = r[3];
+    const double Z = std::max(std::max(cz(o[0][0] - o[2][0], r[0] + r[2]), cz(o[1][0] - o[3][0], r[1] + r[3])),
+                              std::max(cz(o[0][0] - o[3][0], r[0] + r[3]), cz(o[1][0] - o[2][0], r[1] + r[2])));
+    o[2][2] = o[3][2] = Z;
+  } else if (n > 4) {
+    double cur = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+      if (i > 0) cur += r[i - 1] + r[i];
+      o[i][0] = cur;
+    }
+  }
+  if (n) {
+    double lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) { lo[d] = o[0][d] - r[0]; hi[d] = o[0][d] + r[0]; }
+    for (size_t i = 1; i < n; ++i)
+      for (int d = 0; d < 3; ++d) { lo[d] = std::min(lo[d], o[i][d] - r[i]); hi[d] = std::max(hi[d], o[i][d] + r[i]); }
+    for (size_t i = 0; i < n; ++i) {
+      o[i][0] -= 0.5 * (lo[0] + hi[0]);
+      o[i][2] -= 0.5 * (lo[2] + hi[2]);
+    }
+  }
+  return o;
+}
+}  // namespace
+
+pm_status pm_setup_scene_blobs(pm_sim* sim, float fps, const float* color_ratios, const float* latents, uint32_t k,
+                               const char* pigment_config_path, const char* sim_config_path, const char* anim_path) {
+  if (!sim) return fail(PM_ERR_INVALID, "NULL sim");
+  if (k == 0 || !color_ratios || !latents) return fail(PM_ERR_INVALID, "need k >= 1 colour ratios and latents");
+  if (k > 1024) return fail(PM_ERR_INVALID, "at most 1024 blobs");
+  // the configuration first: the particle mass below uses its density
+  pm_status s;
+  if (pigment_config_path && (s = pm_load_pigment_config(sim, pigment_config_path)) != PM_OK) return s;
+  if (sim_config_path && (s = pm_load_sim_config(sim, sim_config_path)) != PM_OK) return s;
+  const double kv = 4.0 * kBlobAspect * std::pow(std::tgamma(1.0 + 1.0 / kBlobExp), 3) / std::tgamma(1.0 + 3.0 / kBlobExp);
+  std::vector<double> R(k), H(k);
+  for (uint32_t i = 0; i < k; ++i) {
+    R[i] = std::cbrt(blob_volume((double)color_ratios[i]) / kv);  // V = kv R^3
+    H[i] = kBlobAspect * R[i];
+  }
+  const auto off = blob_offsets(R);
+  // sampleParticlesFromVdb (sampling_particles_vdb.hpp:87-150): radius 0.01, 27 particles per cell
+  constexpr double kRadius = 0.01, kPpc = 27.0;
+  std::vector<float> x, lat;
+  double box_volume = 0.0;
+  size_t box_samples = 0;
+  for (uint32_t i = 0; i < k; ++i) {
+    const double lo[3] = {off[i][0] - R[i], 0.0, off[i][2] - R[i]};
+    const double L[3] = {2.0 * R[i], H[i], 2.0 * R[i]};
+    uint32_t n = 0;
+    if ((s = pm_sample_particles(sim->device, L[0], L[1], L[2], kRadius, kPpc, 0, 30, 2, 42 + i, nullptr, 0, &n,
+                                 nullptr, nullptr)) != PM_OK)
+      return s;
+    std::vector<float> pts((size_t)n * 3);
+    if ((s = pm_sample_particles(sim->device, L[0], L[1], L[2], kRadius, kPpc, 0, 30, 2, 42 + i, pts.data(), n, &n,
+                                 nullptr, nullptr)) != PM_OK)
+      return s;
+    box_volume += L[0] * L[1] * L[2];
+    box_samples += n;
+    for (uint32_t j = 0; j < n; ++j) {
+      double p[3], f = 0.0;
+      for (int d = 0; d < 3; ++d) p[d] = (double)pts[3 * j + d] + lo[d];
+      const double dxr = (p[0] - off[i][0]) / R[i], dy = p[1] / H[i], dzr = (p[2] - off[i][2]) / R[i];
+      f = std::pow(std::fabs(dxr), kBlobExp) + std::pow(std::fabs(dy), kBlobExp) + std::pow(std::fabs(dzr), kBlobExp);
+      if (!(f <= 1.0 && p[1] >= 0.0)) continue;
+      for (int d = 0; d < 3; ++d) x.push_back((float)p[d]);
+      for (int c = 0; c < 7; ++c) lat.push_back(latents[7 * i + c]);
+    }
+  }
+  if (x.empty()) return fail(PM_ERR_INVALID, "the blobs hold no particles");
+  const double dx = std::cbrt(kPpc / (double)box_samples * box_volume);
+  if ((s = pm_set_particles(sim, (uint32_t)(x.size() / 3), x.data(), lat.data(), nullptr)) != PM_OK) return s;
+  if ((s = setup_scene_common(sim, fps, nullptr, nullptr, anim_path)) != PM_OK) return s;
+  HostParams& h = sim->hp;
+  h.dx = dx;
+  h.particle_volume = dx * dx * dx / kPpc;
+  h.particle_mass = h.rho * h.particle_volume;
   return PM_OK;
 }
 

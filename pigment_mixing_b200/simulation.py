@@ -133,6 +133,19 @@ class Simulation:
         enc = lambda s: None if s is None else s.encode()
         call("pm_setup_scene", self._h, float(fps), enc(pigment_config), enc(sim_config), enc(anim_path))
 
+    def setupSceneBlobs(self, fps: float, color_ratios, latents, pigment_config: Optional[str] = None,
+                        sim_config: Optional[str] = None, anim_path: Optional[str] = None) -> None:
+        """setupScene(fps, colorRatios, pigments, anim_path) with the blob scene built by the library
+        (pm_setup_scene_blobs): one blob per colour ratio, latents[k, 7] their Mixbox latents."""
+        r = _f32(color_ratios).reshape(-1)
+        lat = _f32(latents).reshape(len(r), 7)
+        enc = lambda s: None if s is None else s.encode()  # noqa: E731
+        call("pm_setup_scene_blobs", self._h, float(fps), _fp(r), _fp(lat), len(r), enc(pigment_config),
+             enc(sim_config), enc(anim_path))
+        n = C.c_double()
+        call("pm_get_param", self._h, b"Np", C.byref(n))
+        self._np = int(n.value)
+
     def prepareSimulation(self) -> None:  # simulation_units.cpp:133-215
         call("pm_prepare", self._h)
 

@@ -2,8 +2,8 @@
 
 Run in a container where the reference is mounted (it reads it, the tests never do):
 
-    make -C oracle ref                       # compiles the reference's mixbox.cpp in place
-    python tests/golden/make_golden.py /root/reference
+    make -C oracle ref REF=<reference tree>     # compiles the reference's mixbox.cpp in place
+    python tests/golden/make_golden.py <reference tree>
 
 Writes
   mixbox_latents.json    Mixbox float RGB -> 7-float latent for the scene colours, produced by
@@ -13,6 +13,11 @@ Writes
   spatula_frames_head.npy  the first 481 keyframes (8 s at 60 fps) of the reference's knife
                          animation matter/animations/spatula_motion.bin (7 float32 per frame:
                          position xyz, quaternion xyzw; object_spatula.hpp:7-10).
+  spatula_motion.bin     that animation whole (3,601 frames), byte for byte, for the tests of
+                         pm_add_spatula_file and pm_setup_scene.
+  sim_config.json,       the reference's own configuration files (matter/sim_config.json,
+  pigment_config.json    matter/pigment_config.json), byte for byte, for the tests of the JSON
+                         readers (simulation_units.cpp:31-80).
 """
 import ctypes as C
 import json
@@ -63,8 +68,15 @@ def main(ref_root: str) -> None:
     anim = os.path.join(ref_root, "matter", "animations", "spatula_motion.bin")
     frames = np.fromfile(anim, dtype=np.float32).reshape(-1, 7)
     np.save(os.path.join(HERE, "spatula_frames_head.npy"), frames[:481].copy())
-    print("wrote mixbox_latents.json and spatula_frames_head.npy (%d frames total in source)" % len(frames))
+    for src, dst in ((anim, "spatula_motion.bin"), (os.path.join(ref_root, "matter", "sim_config.json"), "sim_config.json"),
+                     (os.path.join(ref_root, "matter", "pigment_config.json"), "pigment_config.json")):
+        with open(src, "rb") as f, open(os.path.join(HERE, dst), "wb") as g:
+            g.write(f.read())
+    print("wrote mixbox_latents.json, spatula_frames_head.npy, spatula_motion.bin (%d frames), sim_config.json, "
+          "pigment_config.json" % len(frames))
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_golden.py <reference tree>")
+    main(sys.argv[1])
