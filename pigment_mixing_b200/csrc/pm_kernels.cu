@@ -587,6 +587,10 @@ constexpr int kThreads = 128;  // threads per CTA of the brick kernels
 #ifndef PM_G2P_UNROLL_X
 #define PM_G2P_UNROLL_X 3
 #endif
+// 1: the G2P gather's velocity sums in sum-factorised form (rows, then layers, then the stencil).
+#ifndef PM_G2P_FACTORED
+#define PM_G2P_FACTORED 0
+#endif
 #ifndef PM_DEFGRAD_UNROLL_X
 #define PM_DEFGRAD_UNROLL_X 1
 #endif
@@ -650,6 +654,28 @@ struct StencilPoly {
   __device__ __forceinline__ float dN(float f) const { return fmaf(d1, f, d0); }
 };
 
+// Packed FP32 pairs (sm_100): one instruction performs two multiplies, adds or FMAs, each rounded
+// exactly as the scalar instruction, so pair arithmetic gives the bits two scalar instructions give.
+// The scatters stage the x and y parts of their per-particle vectors in adjacent float4 slots so that
+// they load as register pairs.  PM_PACKED=0 compiles the scalar forms instead.
+#ifndef PM_PACKED
+#define PM_PACKED 1
+#endif
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+
+// The x and y axes of a lane's StencilPoly as pairs: N and dN of both axes in one instruction each.
+struct StencilPoly2 {
+  float2 n0, n1, n2, d0, d1;
+  __device__ __forceinline__ StencilPoly2(const StencilPoly& a, const StencilPoly& b)
+      : n0{a.n0, b.n0}, n1{a.n1, b.n1}, n2{a.n2, b.n2}, d0{a.d0, b.d0}, d1{a.d1, b.d1} {}
+  __device__ __forceinline__ float2 N(float2 f) const { return fma2(fma2(n2, f, n1), f, n0); }
+  __device__ __forceinline__ float2 dN(float2 f) const { return fma2(d1, f, d0); }
+};
+
 size_t p2g_smem_bytes() { return sizeof(float) * kP2GCh * kTileStride + sizeof(float4) * kStageP2G * kThreads; }
 
 
@@ -687,6 +713,10 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
   const float D = P.apicD, dx = P.dx;
   const bool apic = P.flip_ratio < 0.f;
   const StencilPoly px(la, P.inv_dx), py(lb, P.inv_dx), pz(lc, P.inv_dx);
+#if PM_PACKED
+  const StencilPoly2 pxy(px, py);
+  const float2 fa2 = dup2(fa), fb2 = dup2(fb), fc2 = dup2(fc);
+#endif
   const int nbr = c->n_bricks;
   for (int b = blk_; b < nbr; b += nblk_) {
     const uint32_t ps = B.cell[(size_t)b * kBrickNodes], pe = B.cell[(size_t)(b + 1) * kBrickNodes];
@@ -727,6 +757,18 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
         for (int k = 0; k < 6; ++k) tau[k] = B.pin[(F_TAU + k) * S + o];
 #pragma unroll
         for (int k = 0; k < 7; ++k) lat[k] = B.pin[(F_LAT + k) * S + o];
+#if PM_PACKED
+        // packed layout: pairs (fx, fy), (q0, q1), (C0x, C0y), (C1x, C1y), (C2x, C2y), (lat0, lat1),
+        // (lat2, lat3), (lat4, lat5), (lat6, diffusion) each in one aligned half of a float4
+        st[0 * 32 + lane] = make_float4(r[0] * P.inv_dx, r[1] * P.inv_dx, r[2] * P.inv_dx, C[2]);
+        st[1 * 32 + lane] = make_float4(q[0], q[1], q[2], C[5]);
+        st[2 * 32 + lane] = make_float4(C[0], C[1], C[3], C[4]);
+        st[3 * 32 + lane] = make_float4(C[6], C[7], C[8], tau[0]);
+        st[4 * 32 + lane] = make_float4(tau[1], tau[2], tau[3], tau[4]);
+        st[5 * 32 + lane] = make_float4(tau[5], 0.f, lat[0], lat[1]);
+        st[6 * 32 + lane] = make_float4(lat[2], lat[3], lat[4], lat[5]);
+        st[7 * 32 + lane] = make_float4(lat[6], B.pin[F_DIFF * S + o], 0.f, 0.f);
+#else
         st[0 * 32 + lane] = make_float4(r[0] * P.inv_dx, r[1] * P.inv_dx, r[2] * P.inv_dx, B.pin[F_DIFF * S + o]);
         st[1 * 32 + lane] = make_float4(q[0], q[1], q[2], lat[0]);
         st[2 * 32 + lane] = make_float4(C[0], C[1], C[2], C[3]);
@@ -735,6 +777,7 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
         st[5 * 32 + lane] = make_float4(tau[3], tau[4], tau[5], lat[1]);
         st[6 * 32 + lane] = make_float4(lat[2], lat[3], lat[4], lat[5]);
         st[7 * 32 + lane] = make_float4(lat[6], 0.f, 0.f, 0.f);
+#endif
       }
       // runs of equal cells among the warp's particles
       const int prev = __shfl_up_sync(0xffffffffu, cl, 1);
@@ -747,6 +790,42 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
         const int cell = __shfl_sync(0xffffffffu, cl, s0);
         if (lane < 27) {
           float acc[kP2GCh];
+#if PM_PACKED
+          // A B-spline weight of a stencil node is never below 1e-16 unless it is exactly 0 (the
+          // particle's offset f from its base cell is a float in [0.5, 1.5), so (f - 1/2)^2 / 2 is 0
+          // or at least about 1.8e-15), so p2g.cpp:39's skip of weights <= 1e-25 only skips terms
+          // that are 0 anyway: the weight is used as is.
+          float2 a_v = make_float2(0.f, 0.f), a_l01 = a_v, a_l23 = a_v, a_l45 = a_v, a_l6s = a_v;
+          float a_m = 0.f, a_vz = 0.f, a_f0 = 0.f, a_f1 = 0.f, a_f2 = 0.f;
+#pragma unroll kScatterUnroll
+          for (int q = s0; q < s1; ++q) {
+            const float4 S0 = st[0 * 32 + q], S1 = st[1 * 32 + q], S2 = st[2 * 32 + q], S3 = st[3 * 32 + q];
+            const float4 S4 = st[4 * 32 + q], S5 = st[5 * 32 + q], S6 = st[6 * 32 + q], S7 = st[7 * 32 + q];
+            const float2 nxy = pxy.N(lo2(S0)), dxy = pxy.dN(lo2(S0));
+            const float nx = nxy.x, ny = nxy.y, nz = pz.N(S0.z);
+            const float nyz = ny * nz;
+            const float w = nx * nyz;
+            const float gx = dxy.x * nyz, gy = nx * dxy.y * nz, gz = nx * ny * pz.dN(S0.z);
+            const float2 w2 = dup2(w);
+            a_m += w;
+            float2 vxy = fma2(fa2, lo2(S2), lo2(S1));
+            vxy = fma2(fb2, hi2(S2), vxy);
+            vxy = fma2(fc2, lo2(S3), vxy);
+            a_v = fma2(w2, vxy, a_v);
+            a_vz += w * (S1.z + fa * S0.w + fb * S1.w + fc * S3.z);
+            a_f0 += S3.w * gx + S4.z * gy + S4.w * gz;
+            a_f1 += S4.z * gx + S4.x * gy + S5.x * gz;
+            a_f2 += S4.w * gx + S5.x * gy + S4.y * gz;
+            a_l01 = fma2(w2, hi2(S5), a_l01);
+            a_l23 = fma2(w2, lo2(S6), a_l23);
+            a_l45 = fma2(w2, hi2(S6), a_l45);
+            a_l6s = fma2(w2, lo2(S7), a_l6s);
+          }
+          acc[0] = a_m; acc[1] = a_v.x; acc[2] = a_v.y; acc[3] = a_vz;
+          acc[4] = a_f0; acc[5] = a_f1; acc[6] = a_f2;
+          acc[7] = a_l01.x; acc[8] = a_l01.y; acc[9] = a_l23.x; acc[10] = a_l23.y;
+          acc[11] = a_l45.x; acc[12] = a_l45.y; acc[13] = a_l6s.x; acc[14] = a_l6s.y;
+#else
 #pragma unroll
           for (int k = 0; k < kP2GCh; ++k) acc[k] = 0.f;
 #pragma unroll kScatterUnroll
@@ -774,6 +853,7 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
             acc[13] += wm * L1.x;
             acc[14] += wm * Fr.w;
           }
+#endif
           const int tp = ((cell >> 4) + la) * kSX + (((cell >> 2) & 3) + lb) * kSY + ((cell & 3) + lc);
 #pragma unroll
           for (int k = 0; k < kP2GCh; ++k)
@@ -1091,8 +1171,6 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float4* st = stw + warp * kStageMUSL * 32;
   const int la = lane / 9, lb = (lane / 3) % 3, lc = lane % 3;
-  const float fa = (float)la, fb = (float)lb, fcc = (float)lc;
-  const StencilPoly px(la, P.inv_dx), py(lb, P.inv_dx), pz(lc, P.inv_dx);
   const float D = P.apicD, dx = P.dx;
   const float fr = P.flip_ratio;
   const bool apic = fr < 0.f, use_flip = kFlip, musl = P.use_musl != 0;
@@ -1146,6 +1224,45 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
         for (int k = 0; k < 6; ++k) Ls[k] = 0.f;
 #pragma unroll
         for (int k = 0; k < 7; ++k) gl[k] = 0.f;
+#if PM_PACKED
+        // latent and shear sums on pairs straight from the tile records: (lat1, lat2), (lat3, lat4),
+        // (lat5, lat6) and (shear, node mass; the mass sum is not used)
+        float2 g12 = make_float2(0.f, 0.f), g34 = g12, g56 = g12, gsm = g12;
+#endif
+#if PM_G2P_FACTORED
+        // Sum factorisation: the weight of node (a, b, c) is Na Nb Nc, so every velocity sum is
+        // formed along each row of three nodes (over c), then over the rows of a layer (b), then
+        // over the layers (a): per row P = sum_c Nc v, Q = sum_c dNc v and Z = sum_c o_c Nc v (o the
+        // node offset -1, 0, 1 from the stencil's middle node); per layer S = sum_b Nb P,
+        // Sd = sum_b dNb P, SQ = sum_b Nb Q, Sz = sum_b Nb Z, Sy = sum_b o_b Nb P; finally
+        // vp = sum_a Na S, the offset sums of B (sum_a o_a Na S, sum_a Na Sy, sum_a Na Sz) and the
+        // velocity gradient's columns L[:, 0] = sum_a dNa S, L[:, 1] = sum_a Na Sd,
+        // L[:, 2] = sum_a Na SQ.  Latent, shear and FLIP sums stay node by node.
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const float Na = aw[0].N[a], dNa = aw[0].dN[a];
+          float Sv[3] = {0.f, 0.f, 0.f}, Sy[3] = {0.f, 0.f, 0.f}, Sz[3] = {0.f, 0.f, 0.f};
+          float Sd[3] = {0.f, 0.f, 0.f}, SQ[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+          for (int bb = 0; bb < 3; ++bb) {
+            const float Nb = aw[1].N[bb], dNb = aw[1].dN[bb];
+            const float nxy = Na * Nb;
+            float Pv[3] = {0.f, 0.f, 0.f}, Qv[3] = {0.f, 0.f, 0.f}, Zv[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int cz = 0; cz < 3; ++cz) {
+              const int tn = ((lx + a) * kTile + (ly + bb)) * kTile + (lz + cz);
+              const float Nc = aw[2].N[cz], dNc = aw[2].dN[cz];
+              const float4 R0 = tile[tn], R1 = tile[kG2PTileStride + tn], R2 = tile[2 * kG2PTileStride + tn];
+              const float gv[3] = {R0.x, R0.y, R0.z};
+#pragma unroll
+              for (int r = 0; r < 3; ++r) {
+                Pv[r] += Nc * gv[r];
+                Qv[r] += dNc * gv[r];
+                if (cz == 0) Zv[r] -= Nc * gv[r];
+                if (cz == 2) Zv[r] += Nc * gv[r];
+              }
+              const float w = nxy * Nc;
+#else
 #pragma unroll kG2PUnrollX
         for (int a = 0; a < 3; ++a) {
           const float oa = (float)(a - 1);
@@ -1176,17 +1293,58 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
               Ls[3] += gv[0] * g1 + gv[1] * g0;
               Ls[4] += gv[0] * g2 + gv[2] * g0;
               Ls[5] += gv[1] * g2 + gv[2] * g1;
+#endif
               if (use_flip) {
                 const float4 R3 = tile[3 * kG2PTileStride + tn];
                 fp[0] += R3.x * w; fp[1] += R3.y * w; fp[2] += R3.z * w;
               }
               gl[0] += R0.w * w;
+#if PM_PACKED
+              const float2 w2 = dup2(w);
+              g12 = fma2(w2, lo2(R1), g12);
+              g34 = fma2(w2, hi2(R1), g34);
+              g56 = fma2(w2, lo2(R2), g56);
+              gsm = fma2(w2, hi2(R2), gsm);
+#else
               gl[1] += R1.x * w; gl[2] += R1.y * w; gl[3] += R1.z * w; gl[4] += R1.w * w;
               gl[5] += R2.x * w; gl[6] += R2.y * w;
               gs += R2.z * w;
+#endif
             }
+#if PM_G2P_FACTORED
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+              Sv[r] += Nb * Pv[r];
+              Sd[r] += dNb * Pv[r];
+              SQ[r] += Nb * Qv[r];
+              Sz[r] += Nb * Zv[r];
+              if (bb == 0) Sy[r] -= Nb * Pv[r];
+              if (bb == 2) Sy[r] += Nb * Pv[r];
+            }
+#endif
           }
+#if PM_G2P_FACTORED
+#pragma unroll
+          for (int r = 0; r < 3; ++r) {
+            vp[r] += Na * Sv[r];
+            if (a == 0) Bp[3 * r] -= Na * Sv[r];
+            if (a == 2) Bp[3 * r] += Na * Sv[r];
+            Bp[3 * r + 1] += Na * Sy[r];
+            Bp[3 * r + 2] += Na * Sz[r];
+          }
+          // L[r][k] = sum v_r d_k w: column 0 sum_a dNa S, column 1 sum_a Na Sd, column 2 sum_a Na SQ
+          Ls[0] += dNa * Sv[0];
+          Ls[1] += Na * Sd[1];
+          Ls[2] += Na * SQ[2];
+          Ls[3] += dNa * Sv[1] + Na * Sd[0];
+          Ls[4] += dNa * Sv[2] + Na * SQ[0];
+          Ls[5] += Na * (Sd[2] + SQ[1]);
+#endif
         }
+#if PM_PACKED
+        gl[1] = g12.x; gl[2] = g12.y; gl[3] = g34.x; gl[4] = g34.y; gl[5] = g56.x; gl[6] = g56.y;
+        gs = gsm.x;
+#endif
         // B = sum w v (x_i - x_p)^T, accumulated above with the node offsets o in {-1, 0, 1} from
         // the stencil's middle node (x_i - x_p = o dx - (r - dx)): B = dx sum w v o^T - (sum w v)
         // (r - dx)^T.  Centring keeps both terms within half a cell (r - dx is exact), so their
@@ -1245,10 +1403,18 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
           for (int k = 0; k < 3; ++k)
 #pragma unroll
             for (int qq = 0; qq < 3; ++qq) C[3 * k + qq] = D * dx * Bp[3 * qq + k];
+#if PM_PACKED
+          // packed layout: pairs (fx, fy), (q0, q1), (C0x, C0y), (C1x, C1y), (C2x, C2y)
+          st[0 * 32 + lane] = make_float4(r3[0] * P.inv_dx, r3[1] * P.inv_dx, r3[2] * P.inv_dx, q[2]);
+          st[1 * 32 + lane] = make_float4(q[0], q[1], C[2], C[5]);
+          st[2 * 32 + lane] = make_float4(C[0], C[1], C[3], C[4]);
+          st[3 * 32 + lane] = make_float4(C[6], C[7], C[8], 0.f);
+#else
           st[0 * 32 + lane] = make_float4(q[0], q[1], q[2], r3[0] * P.inv_dx);
           st[1 * 32 + lane] = make_float4(C[0], C[1], C[2], C[3]);
           st[2 * 32 + lane] = make_float4(C[4], C[5], C[6], C[7]);
           st[3 * 32 + lane] = make_float4(C[8], r3[1] * P.inv_dx, r3[2] * P.inv_dx, 0.f);
+#endif
         }
       }
       if (musl) {
@@ -1261,7 +1427,31 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
           const int s1 = heads ? __ffs(heads) - 1 : n;
           const int cell = __shfl_sync(0xffffffffu, cl, s0);
           if (lane < 27) {
+            // the lane's stencil node constants, formed here so that they are not live across the
+            // gather above
+            const float fa = (float)la, fb = (float)lb, fcc = (float)lc;
+            const StencilPoly px(la, P.inv_dx), py(lb, P.inv_dx), pz(lc, P.inv_dx);
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#if PM_PACKED
+            const StencilPoly2 pxy(px, py);
+            const float2 fa2 = dup2(fa), fb2 = dup2(fb), fc2 = dup2(fcc);
+            // weights as in P2G (the skip of weights <= 1e-25, musl.cpp:188, only skips zeros)
+            float2 a_v = make_float2(0.f, 0.f);
+#pragma unroll kScatterUnroll
+            for (int q = s0; q < s1; ++q) {
+              const float4 S0 = st[0 * 32 + q], S1 = st[1 * 32 + q], S2 = st[2 * 32 + q], S3 = st[3 * 32 + q];
+              const float2 nxy = pxy.N(lo2(S0));
+              const float w = nxy.x * (nxy.y * pz.N(S0.z));
+              float2 vxy = fma2(fa2, lo2(S2), lo2(S1));
+              vxy = fma2(fb2, hi2(S2), vxy);
+              vxy = fma2(fc2, lo2(S3), vxy);
+              a_v = fma2(dup2(w), vxy, a_v);
+              acc[2] += w * (S0.w + fa * S1.z + fb * S1.w + fcc * S3.z);
+              acc[3] += w;
+            }
+            acc[0] = a_v.x;
+            acc[1] = a_v.y;
+#else
 #pragma unroll kScatterUnroll
             for (int q = s0; q < s1; ++q) {
               const float4 Q = st[0 * 32 + q], C0 = st[1 * 32 + q], C1 = st[2 * 32 + q], C2 = st[3 * 32 + q];
@@ -1272,6 +1462,7 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
               acc[2] += wm * (Q.z + fa * C0.z + fb * C1.y + fcc * C2.x);
               acc[3] += wm;
             }
+#endif
             const int tp = ((cell >> 4) + la) * kSX + (((cell >> 2) & 3) + lb) * kSY + ((cell & 3) + lc);
 #pragma unroll
             for (int k = 0; k < 4; ++k) atomicAdd(&mtile[k * kTileStride + tp], acc[k]);
