@@ -249,14 +249,19 @@ def drift(scene, steps, device=0):
     torch.cuda.synchronize(device)
     ev[0].record(stream)
     done = 0
+    seg_state = []
     for j in range(1, len(ev)):
         k = min(seg, steps - done)
         g.advance(k)
         done += k
         ev[j].record(stream)
+        rm = g.returnMapStats()  # the last step of the segment (waits for it)
+        seg_state.append({"plastic": int(g.plastic_count), "newton_solves": rm["solves"],
+                          "newton_updates": rm["newton_iters"], "grid_nodes": int(g.grid_nodes)})
     torch.cuda.synchronize(device)
     ms = ev[0].elapsed_time(ev[-1])
     seg_ms = [ev[j - 1].elapsed_time(ev[j]) / seg for j in range(1, len(ev))]
+    late = {k: round(v * 1e3, 1) for k, v in g.profileSteps(5).items()}  # us per kernel, after the run
     s1 = g.stats()
     flags = g.errorFlags()
     nodes = int(g.grid_nodes)
@@ -264,6 +269,7 @@ def drift(scene, steps, device=0):
               "capacity_nodes_end": int(g.grid_capacity_nodes)}
     g.close()
     return {"steps": steps, "ms_per_step_avg": ms / steps, "ms_per_step_by_segment": seg_ms,
+            "state_by_segment": seg_state, "kernel_us_after_run": late,
             "particle_steps_per_s": len(scene["x"]) * steps / (ms / 1e3),
             "mass_rel": abs(s1["mass"] - s0["mass"]) / s0["mass"],
             "mean_latent_abs": float(np.abs(s1["mean_latent"] - s0["mean_latent"]).max()),
@@ -337,7 +343,15 @@ def run_ours(args):
     g = sim.grid()
     active_nodes = int((g["mass"] > 0).sum())
     kps = int(sim.kernels_per_step)
-    kms = sim.profileSteps(5)
+    sim.close()
+    # per-kernel times over the same steps as the timed region: a fresh simulation of the scene
+    # after the same warm-up, every kernel of its K steps timed with CUDA events on its stream
+    prof = Simulation(device)
+    scenes.apply(scene, prof)
+    prof.prepareSimulation()
+    prof.advance(args.warmup)
+    kms = prof.profileSteps(args.steps)
+    prof.close()
     dom = max((k for k in kms if k in ALGO_BYTES), key=lambda k: kms[k])
     peak, peak_kind = _peaks()
     pb, nb = ALGO_BYTES[dom]
@@ -351,7 +365,7 @@ def run_ours(args):
             "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"}
     step_roof = {"bytes": step_bytes, "achieved": step_bytes / (step_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                  "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak, "active_nodes": active_nodes}
-    sim.close()
+    roof["timed_over"] = f"the {args.steps} steps after {args.warmup} warm-up steps (a second run of the timed steps)"
     sur = None
     if not args.no_surrogate:
         sur = _surrogate_leg(scene, args, device, dist, ws, value, x_ref, lat_ref, newton_plain)
@@ -361,6 +375,8 @@ def run_ours(args):
     batch = None
     if not args.no_batch:
         batch = _batch_leg(args, device, dist, ws)
+        if sur is not None:
+            batch["surrogate"] = _batch_leg(args, device, dist, ws, sur["_params"])
     # -------- end to end through the C ABI from pinned host buffers --------
     _e2e(scene, args, device, dist, ws)  # untimed pass: first-use costs of the API path (allocator, streams)
     # three timed passes, the median reported: one pass is about a tenth of a second of host and
@@ -369,24 +385,38 @@ def run_ours(args):
     e2e = dict(runs[1])
     e2e["passes"] = [r["value"] for r in runs]
     e2e["includes"] += "; median of three timed passes"
+    if rank == 0:
+        e2e["breakdown"] = _e2e_breakdown(scene, args, device)
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": _config(scene, args),
             "roofline": roof, "step_roofline": step_roof, "e2e": e2e, "clocks": clocks,
             "gpu_launches": args.steps * kps,
             "kernel_ms": kms, "error_flags": flags}
+    sur_params = None
     if sur is not None:
+        sur_params = sur.pop("_params")
         line["surrogate"] = sur
+    if rank == 0 and ws == 1 and args.workload == "2m" and not args.no_big:
+        line["point_8m"] = _big_point(args, device, sur_params)
     if batch is not None:
         line["batch"] = batch
     if splat is not None:
         line["splat"] = splat
     if args.drift_steps > 0:
         line["drift"] = drift(scene, args.drift_steps, device)
+        d = line["drift"]
+        line["full_run"] = {"steps": d["steps"], "value": d["particle_steps_per_s"], "unit": METRIC,
+                            "ms_per_step": d["ms_per_step_avg"],
+                            "note": "the workload's full step count from a fresh start (drift leg); the plastic "
+                                    "particle count and Newton updates per solve grow as the knife works the paint"}
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline(scene).items() if k != "seconds"}
         # the FP64 oracle as checker: 50-step error on the 32,768-particle scene of the same recipe
         line["accuracy"] = accuracy_vs_oracle(_workload("32k"), 50, _small_surrogate(device), device)
+        if args.workload == "2m" and not args.no_accuracy_2m:
+            # the headline scene itself: 50 steps of the FP64 oracle (all host threads) as the checker
+            line["accuracy_2m"] = accuracy_vs_oracle(scene, 50, sur_params, device)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -396,7 +426,7 @@ def run_ours(args):
 def _ncu_traffic(kernel):
     """dram__bytes_read.sum + dram__bytes_write.sum per launch of ``kernel`` from the committed ncu
     summary of the 2M scene (line ``traffic_bytes_per_launch: name=bytes ...``)."""
-    path = os.path.join(ROOT, "profiles", "k_p2g_g2p_defgrad_2m_full.md")
+    path = os.path.join(ROOT, "profiles", "dram_traffic_transfer_kernels_2m.md")
     try:
         with open(path) as f:
             for line in f:
@@ -461,13 +491,32 @@ def _surrogate_leg(scene, args, device, dist, ws, plain_value, x_ref, lat_ref, n
     newton_sur = _newton_per_solve(s, 4)
     kms = s.profileSteps(3)
     s.close()
-    return {"value": value, "unit": METRIC, "ms_per_step": ms / args.steps, "speedup_vs_plain": value / plain_value,
+    st = _rm_stats_after(scene, params, device)
+    return {"_params": params, "value": value, "unit": METRIC, "ms_per_step": ms / args.steps,
+            "speedup_vs_plain": value / plain_value, "acceptance": st,
             "train": {"samples": int(len(xs)), "logged_steps": args.log_steps, "log_every": every, "epochs": args.train_epochs,
                       "seconds": train_s, "loss_first_epoch": float(hist[0]), "loss_last_epoch": float(hist[-1])},
             "newton": {"plain": newton_plain, "surrogate": newton_sur},
             "max_position_diff_vs_plain": dx, "max_latent_diff_vs_plain": dl,
             "kernel_ms": {k: kms[k] for k in ("k_defgrad_head", "k_defgrad_tail", "k_mlp_infer", "k_sur_finish")
                           if k in kms}}
+
+
+def _rm_stats_after(scene, params, device, steps=10):
+    """Return-map statistics of the surrogate form after a few steps of the scene: particles sent to
+    the network, estimates that passed the consistency check, and the fallback rate."""
+    from pigment_mixing_b200 import RETURN_MAP_SURROGATE, Simulation, scenes
+    s = Simulation(device)
+    scenes.apply(scene, s)
+    s.setSurrogate(params)
+    s.setReturnMap(RETURN_MAP_SURROGATE)
+    s.prepareSimulation()
+    s.advance(steps)
+    st = s.returnMapStats()
+    s.close()
+    return {"after_steps": steps, "queued": st["queued"], "accepted": st["accepted"],
+            "fallback_rate": 1.0 - st["accepted"] / max(1, st["queued"]),
+            "newton_updates": st["newton_iters"], "solves": st["solves"]}
 
 
 def _small_surrogate(device):
@@ -484,13 +533,14 @@ def _small_surrogate(device):
     return params
 
 
-def _batch_leg(args, device, dist, ws):
+def _batch_leg(args, device, dist, ws, params=None):
     """The batched workload: args.batch_scenes independent palette scenes (particle counts
     log-uniform 20k-400k, grids 64^3-160^3, random pigment pair, yield and knife path) stepped
     together through pm_batch (autotuned launch shapes, one CUDA graph per round), against the
-    same scenes advanced one after another through the single-scene API."""
+    same scenes advanced one after another through the single-scene API.  With params, every
+    scene runs the learned return map (the surrogate form)."""
     import torch
-    from pigment_mixing_b200 import Batch, Simulation, scenes
+    from pigment_mixing_b200 import RETURN_MAP_SURROGATE, Batch, Simulation, scenes
     scs = scenes.batch_scenes(args.batch_scenes, seed=0)
     npart = sum(len(sc["x"]) for sc in scs)
 
@@ -499,6 +549,9 @@ def _batch_leg(args, device, dist, ws):
         for sc in scs:
             g = Simulation(device)
             scenes.apply(sc, g)
+            if params is not None:
+                g.setSurrogate(params)
+                g.setReturnMap(RETURN_MAP_SURROGATE)
             g.prepareSimulation()
             out.append(g)
         return out
@@ -542,15 +595,20 @@ def _batch_leg(args, device, dist, ws):
     seq_value = ws * npart * args.batch_steps / seq_s
     counts = [len(sc["x"]) for sc in scs]
     grids = [int(round(1.0 / sc["params"]["dx"])) for sc in scs]
-    return {"value": value, "unit": METRIC, "scenes": len(scs), "particles": npart,
+    kernel_sum = sum(prof.values())
+    return {"value": value, "unit": METRIC, "form": "surrogate" if params is not None else "plain",
+            "scenes": len(scs), "particles": npart,
             "particles_min_max": [min(counts), max(counts)], "grid_min_max": [min(grids), max(grids)],
-            "rounds": args.batch_steps, "ms_per_round": ms / args.batch_steps, "tuning": tuning,
+            "rounds": args.batch_steps, "ms_per_round": ms / args.batch_steps,
+            "kernel_ms_sum_per_round": kernel_sum,
+            "launch_gaps_ms_per_round": ms / args.batch_steps - kernel_sum,
+            "tuning": tuning,
             "autotune_ms_per_round": tuned_ms, "autotune_seconds": tune_s,
             "sequential_value": seq_value, "speedup_vs_sequential": value / seq_value,
             "timed_steps": [pre_steps, pre_steps + args.batch_steps],
             "steps_after": steps, "error_flags": flags, "kernel_ms": prof,
             "workload": "palette scenes: 2 blocks each, random pigment pair of 6 RGB seeds, yield U(50,200) Pa, "
-                        "random 3-segment knife path, VMVisc, MUSL, APIC, plain return map"}
+                        "random 3-segment knife path, VMVisc, MUSL, APIC"}
 
 
 def _splat_leg(scene, args, device, dist, with_cpu: bool):
@@ -672,6 +730,106 @@ def _e2e(scene, args, device, dist, ws):
                         "with the following steps), final readback; after one untimed pass"}
 
 
+def _e2e_breakdown(scene, args, device):
+    """One more end-to-end pass, synchronised at every phase boundary, itemising its host time:
+    creation, particle upload (of which buffer allocation), parameters and objects, prepare (of
+    which grid allocation), the K steps (of which step-graph capture and instantiation, and the
+    device time of the steps themselves), the final readback.  Synchronising removes the overlap
+    of the timed passes, so the items add up to a little more than a timed pass."""
+    import torch
+    from pigment_mixing_b200 import Simulation
+    n = len(scene["x"])
+    hx = torch.from_numpy(np.ascontiguousarray(scene["x"], np.float32)).pin_memory()
+    hl = torch.from_numpy(np.ascontiguousarray(scene["latent"], np.float32)).pin_memory()
+    ox = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    ol = torch.empty((n, 7), dtype=torch.float32).pin_memory()
+    od = torch.empty((n,), dtype=torch.float32).pin_memory()
+    t = [time.perf_counter()]
+
+    def mark():
+        torch.cuda.synchronize(device)
+        t.append(time.perf_counter())
+    sim = Simulation(device)
+    mark()
+    sim.setParticles(hx.numpy(), hl.numpy())
+    mark()
+    alloc_upload = float(sim.alloc_ms)
+    sim.set(**scene["params"])
+    for k, v in scene["vectors"].items():
+        setattr(sim, k, v)
+    for kind, kw in scene["objects"]:
+        if kind == "plate":
+            sim.addPlate(kw["pos"], kw["plate_type"], kw["bc"], kw["friction"])
+        elif kind == "box_knife":
+            sim.addBoxKnife(kw["bc"], kw["friction"], kw["half"], kw["waypoints"], kw["speed"])
+    mark()
+    sim.prepareSimulation()
+    mark()
+    alloc_prepare = float(sim.alloc_ms) - alloc_upload
+    stream = torch.cuda.ExternalStream(sim.stream(), device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.advance(args.steps)
+    e1.record(stream)
+    mark()
+    sim.readIntoAsync(x=ox.numpy(), latent=ol.numpy(), diffusion=od.numpy())
+    sim.waitReadback()
+    mark()
+    graph = float(sim.graph_ms)
+    sim.close()
+    ms = [1e3 * (t[i + 1] - t[i]) for i in range(len(t) - 1)]
+    return {"create_ms": ms[0], "upload_ms": ms[1], "upload_alloc_ms": alloc_upload, "setup_ms": ms[2],
+            "prepare_ms": ms[3], "prepare_alloc_ms": alloc_prepare, "steps_ms": ms[4],
+            "steps_graph_build_ms": graph, "steps_device_ms": e0.elapsed_time(e1), "readback_ms": ms[5],
+            "readback_bytes": (ox.numel() + ol.numel() + od.numel()) * 4, "total_ms": sum(ms)}
+
+
+def _big_point(args, device, params):
+    """The 8,388,608-particle scene (four 64^3-cell blocks of four pigments at dx = 1/384): plain and
+    surrogate forms, device-timed like the headline, with the surrogate's acceptance and its
+    difference from the plain path after the same steps."""
+    import torch
+    from pigment_mixing_b200 import RETURN_MAP_SURROGATE, Simulation, scenes
+    sc = _workload("8m")
+    n = len(sc["x"])
+    out = {"workload": sc["name"], "particles": n, "steps": args.steps}
+    ref = None
+    for form in ("plain", "surrogate"):
+        if form == "surrogate" and params is None:
+            break
+        s = Simulation(device)
+        scenes.apply(sc, s)
+        if form == "surrogate":
+            s.setSurrogate(params)
+            s.setReturnMap(RETURN_MAP_SURROGATE)
+        s.prepareSimulation()
+        s.advance(args.warmup)
+        stream = torch.cuda.ExternalStream(s.stream(), device=device)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.advance(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1)
+        st = s.returnMapStats()
+        p = s.getParticles(fields=("x", "latent"))
+        d = {"value": n * args.steps / (ms / 1e3), "unit": METRIC, "ms_per_step": ms / args.steps,
+             "newton_solves_last_step": st["solves"], "newton_updates_last_step": st["newton_iters"]}
+        if form == "surrogate":
+            d["surrogate_queued_last_step"] = st["queued"]
+            d["surrogate_accepted_last_step"] = st["accepted"]
+            d["fallback_rate"] = 1.0 - st["accepted"] / max(1, st["queued"])
+            d["max_position_diff_vs_plain"] = float(np.abs(p.x.astype(np.float64) - ref[0]).max())
+            d["max_latent_diff_vs_plain"] = float(np.abs(p.latent.astype(np.float64) - ref[1]).max())
+            d["speedup_vs_plain"] = d["value"] / out["plain"]["value"]
+        else:
+            ref = (p.x.astype(np.float64), p.latent.astype(np.float64))
+        out[form] = d
+        s.close()
+    return out
+
+
 def profile_run(args):
     """A fixed step sequence for profiler captures: `--warm` steps through advance() (graphs),
     `--profile` steps timed kernel by kernel with CUDA events (printed as JSON), then `--plain`
@@ -718,6 +876,8 @@ def main():
     ap.add_argument("--no-splat", action="store_true", help="skip the pigment-splat leg")
     ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=50, help="timed rounds of the batched leg")
+    ap.add_argument("--no-big", action="store_true", help="skip the 8M-particle point")
+    ap.add_argument("--no-accuracy-2m", action="store_true", help="skip the FP64-oracle check of the 2M scene")
     ap.add_argument("--drift-steps", type=int, default=1000,
                     help="steps of the mass / mean-latent drift run on the workload (0 = skip)")
     args = ap.parse_args()

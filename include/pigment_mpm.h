@@ -63,6 +63,11 @@ typedef enum pm_return_map { PM_RETURN_MAP_PLAIN = 0, PM_RETURN_MAP_SURROGATE = 
 PM_API pm_status pm_create(int device, pm_sim** out);
 /* ~Simulation() */
 PM_API pm_status pm_destroy(pm_sim* sim);
+/* The particle and grid buffers of every simulation on a device come from one pool that keeps
+ * freed memory for the process (as a caching allocator does), so that a later simulation reuses
+ * it without driver allocations.  This hands cached memory above keep_bytes back to the driver
+ * (no counterpart in the reference, which allocates host vectors). */
+PM_API pm_status pm_trim_memory(int device, uint64_t keep_bytes);
 /* Text of the last error on this thread (static storage, never NULL). */
 PM_API const char* pm_last_error_message(void);
 
@@ -78,7 +83,9 @@ PM_API pm_status pm_initialize_basic(pm_sim* sim, const char* name);
  * counterpart) "surrogate_fallback_plain", "sample_log_every".
  * Read-only extras for pm_get_param: "time", "dt", "step", "Np", "mu", "lambda", "K", "dt_max",
  * "frame_dt", "final_time", "n_active", "plastic_count", "grid_nodes", "kernels_per_step",
- * "regrowths", "regrow_ms", "grid_capacity_nodes". */
+ * "regrowths", "regrow_ms", "grid_capacity_nodes", and the host time of a simulation's fixed costs so
+ * far, "alloc_ms" (particle and grid buffer allocation) and "graph_ms" (step-graph capture and
+ * instantiation). */
 PM_API pm_status pm_set_param(pm_sim* sim, const char* name, double value);
 PM_API pm_status pm_get_param(pm_sim* sim, const char* name, double* value);
 /* Vector fields: "gravity", "particle_boundary_min", "particle_boundary_max", "grid_reference_point". */
@@ -233,7 +240,8 @@ PM_API pm_status pm_mlp_infer(const float* params, const float* x, uint32_t n, f
 PM_API pm_status pm_get_stream(pm_sim* sim, void** stream);
 /* Name of the i-th kernel of this simulation's step (launch order), "" when out of range. */
 PM_API const char* pm_kernel_name(pm_sim* sim, int index);
-/* Runs nsteps ordinary steps (no graph), timing every kernel with CUDA events on the stream;
+/* Runs nsteps steps of pm_advance (frame bookkeeping after each) without graphs, timing every
+ * kernel with CUDA events on the stream;
  * kernel_ms[i] receives the mean duration of kernel i.  n_kernels must be >= the kernels per
  * step (pm_get_param "kernels_per_step"). */
 PM_API pm_status pm_profile_steps(pm_sim* sim, uint32_t nsteps, float* kernel_ms, uint32_t n_kernels);

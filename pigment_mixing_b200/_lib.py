@@ -22,6 +22,7 @@ _u8p = C.POINTER(C.c_uint8)
 SIGNATURES = {
     "pm_create": [C.c_int, C.POINTER(C.c_void_p)],
     "pm_destroy": [_vp],
+    "pm_trim_memory": [C.c_int, C.c_uint64],
     "pm_initialize_basic": [_vp, C.c_char_p],
     "pm_set_param": [_vp, C.c_char_p, C.c_double],
     "pm_get_param": [_vp, C.c_char_p, _dp],

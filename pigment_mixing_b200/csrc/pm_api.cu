@@ -172,6 +172,9 @@ struct pm_sim {
 
   bool prepared = false;
   uint32_t host_step = 0;  // steps completed (mirror of ctrl.step after the last sync)
+  // host time spent allocating particle and grid buffers, and capturing and instantiating the
+  // step graphs (pm_get_param "alloc_ms", "graph_ms": the fixed costs of a fresh simulation)
+  double alloc_ms = 0.0, graph_ms = 0.0;
   Params P{};
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   bool graphs_dirty = true;
@@ -208,6 +211,50 @@ struct pm_sim {
   void free_surrogate_queue();
   pm_status ensure_surrogate_queue();
 };
+
+// ------------------------------------------------------------------------------------------
+// Device memory of the particle and grid buffers comes from one stream-ordered pool per device
+// that keeps freed memory for the process (release threshold unlimited), as a caching allocator
+// does: a simulation created after another one has been destroyed (or has shrunk) takes its
+// buffers from the pool instead of the driver, whose large allocations cost milliseconds per
+// gigabyte.  pm_trim_memory returns the cached memory.
+// ------------------------------------------------------------------------------------------
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[64] = {};
+
+cudaError_t pool_of(int device, cudaMemPool_t* out) {
+  if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pool[device]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t p = nullptr;
+    cudaError_t e = cudaMemPoolCreate(&p, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = UINT64_MAX;
+    e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) { cudaMemPoolDestroy(p); return e; }
+    g_pool[device] = p;
+  }
+  *out = g_pool[device];
+  return cudaSuccess;
+}
+
+// Stream-ordered allocation from the device's pool (usable on `s` at once, on other streams once
+// `s` has reached this point).
+cudaError_t pool_alloc(void** ptr, size_t bytes, int device, cudaStream_t s) {
+  cudaMemPool_t p = nullptr;
+  cudaError_t e = pool_of(device, &p);
+  if (e != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(ptr, std::max<size_t>(bytes, 256), p, s);
+}
+template <class T> cudaError_t pool_alloc(T** ptr, size_t bytes, int device, cudaStream_t s) {
+  return pool_alloc(reinterpret_cast<void**>(ptr), bytes, device, s);
+}
+}  // namespace
 
 pm_sim::~pm_sim() {
   if (copy_pending) cudaEventSynchronize(ev_copied);
@@ -255,44 +302,47 @@ void pm_sim::drop_graphs() {
 }
 
 void pm_sim::free_grid() {
-  if (d_cell) cudaFree(d_cell);
-  if (d_scan_part) cudaFree(d_scan_part);
-  if (d_grid) cudaFree(d_grid);
-  if (d_gmusl) cudaFree(d_gmusl);
-  if (d_btouch) cudaFree(d_btouch);
+  for (void* p : {(void*)d_cell, (void*)d_scan_part, (void*)d_grid, (void*)d_gmusl, (void*)d_btouch})
+    if (p) cudaFreeAsync(p, stream);
   d_cell = nullptr; d_scan_part = nullptr; d_grid = nullptr; d_gmusl = nullptr; d_btouch = nullptr;
   brick_cap = 0;
 }
 
 void pm_sim::free_particles() {
   for (int k = 0; k < 2; ++k) {
-    if (d_pbuf[k]) cudaFree(d_pbuf[k]);
-    if (d_meta[k]) cudaFree(d_meta[k]);
+    if (d_pbuf[k]) cudaFreeAsync(d_pbuf[k], stream);
+    if (d_meta[k]) cudaFreeAsync(d_meta[k], stream);
     d_pbuf[k] = nullptr; d_meta[k] = nullptr;
   }
-  if (d_pic) cudaFree(d_pic);
-  if (d_key) cudaFree(d_key);
-  if (d_rank) cudaFree(d_rank);
-  if (d_sorted) cudaFree(d_sorted);
-  if (d_unperm) cudaFree(d_unperm);
-  if (d_active) cudaFree(d_active);
+  for (void* p : {(void*)d_pic, (void*)d_key, (void*)d_rank, (void*)d_sorted, (void*)d_unperm, (void*)d_active})
+    if (p) cudaFreeAsync(p, stream);
   d_pic = nullptr; d_key = d_rank = d_sorted = nullptr; d_unperm = nullptr; d_active = nullptr;
 }
 
+// Adds the host time of its scope to a millisecond counter.
+struct ScopeMs {
+  double& acc;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  explicit ScopeMs(double& a) : acc(a) {}
+  ~ScopeMs() { acc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
 pm_status pm_sim::alloc_grid(int bricks) {
+  ScopeMs timer(alloc_ms);
   drop_graphs();
   free_grid();
   const size_t nodes = (size_t)bricks * kBrickNodes;
   if (nodes + 2 > 0x7fffffffULL) return fail(PM_ERR_CAPACITY, "grid capacity exceeds 2^31 nodes");
-  CK(cudaMalloc(&d_cell, (nodes + 2) * sizeof(uint32_t)));
+  CK(pool_alloc(&d_cell, (nodes + 2) * sizeof(uint32_t), device, stream));
   const size_t scan_blocks = (nodes + 1 + 4095) / 4096 + 1;
-  CK(cudaMalloc(&d_scan_part, scan_blocks * sizeof(uint32_t)));
-  CK(cudaMalloc(&d_grid, nodes * 4 * sizeof(float4)));
-  CK(cudaMalloc(&d_gmusl, nodes * sizeof(float4)));
+  CK(pool_alloc(&d_scan_part, scan_blocks * sizeof(uint32_t), device, stream));
+  CK(pool_alloc(&d_grid, nodes * 4 * sizeof(float4), device, stream));
+  CK(pool_alloc(&d_gmusl, nodes * sizeof(float4), device, stream));
   // grid records need no zeroing here: each step zeroes the bricks it touches (k_clear_bricks)
   // and readers see only touched bricks
-  CK(cudaMalloc(&d_btouch, (size_t)bricks));
+  CK(pool_alloc(&d_btouch, (size_t)bricks, device, stream));
   CK(cudaMemsetAsync(d_btouch, 0, (size_t)bricks, stream));
+  CK(cudaStreamSynchronize(stream));  // the buffers are complete for every stream from here
   brick_cap = bricks;
   return PM_OK;
 }
@@ -386,6 +436,7 @@ pm_status pm_sim::push_ctrl() {
 }
 
 pm_status pm_sim::capture_graphs() {
+  ScopeMs timer(graph_ms);
   drop_graphs();
   for (int start = 0; start < 2; ++start) {
     cudaGraph_t g = nullptr;
@@ -501,6 +552,20 @@ pm_status pm_destroy(pm_sim* sim) {
   cudaSetDevice(sim->device);
   if (sim->stream) cudaStreamSynchronize(sim->stream);
   delete sim;
+  return PM_OK;
+}
+
+pm_status pm_trim_memory(int device, uint64_t keep_bytes) {
+  cudaMemPool_t p = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (device < 0 || device >= 64) return fail(PM_ERR_INVALID, "device ordinal out of range");
+    p = g_pool[device];
+  }
+  if (!p) return PM_OK;
+  CK(cudaSetDevice(device));
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemPoolTrimTo(p, (size_t)keep_bytes));
   return PM_OK;
 }
 
@@ -630,6 +695,8 @@ pm_status pm_get_param(pm_sim* sim, const char* name, double* out) {
   else if (k == "dt_max") *out = sim->P.dt_max;
   else if (k == "frame_dt") *out = sim->P.frame_dt;
   else if (k == "final_time") *out = sim->P.final_time;
+  else if (k == "alloc_ms") *out = sim->alloc_ms;
+  else if (k == "graph_ms") *out = sim->graph_ms;
   else return fail(PM_ERR_INVALID, "unknown parameter " + k);
   return PM_OK;
 }
@@ -717,7 +784,7 @@ pm_status pm_set_particles(pm_sim* sim, uint32_t n, const float* x, const float*
   // stage the host arrays on the device (d_unperm holds n*42 floats >= n*13) and scatter them
   // into the structure-of-arrays state there; the staging buffer comes first so that the copies
   // (asynchronous from pinned host memory) run while the other buffers are allocated
-  CK(cudaMalloc(&sim->d_unperm, (size_t)std::max(n, 1u) * F_COUNT * sizeof(float)));
+  CK(pool_alloc(&sim->d_unperm, (size_t)std::max(n, 1u) * F_COUNT * sizeof(float), sim->device, sim->stream));
   float* dx_ = sim->d_unperm;
   float* dl_ = dx_ + (size_t)n * 3;
   float* dv_ = dl_ + (size_t)n * 7;
@@ -726,15 +793,20 @@ pm_status pm_set_particles(pm_sim* sim, uint32_t n, const float* x, const float*
     if (latent) CK(cudaMemcpyAsync(dl_, latent, (size_t)n * 7 * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
     if (v) CK(cudaMemcpyAsync(dv_, v, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, sim->stream));
   }
-  for (int k = 0; k < 2; ++k) {
-    CK(cudaMalloc(&sim->d_pbuf[k], S * F_COUNT * sizeof(float)));
-    CK(cudaMalloc(&sim->d_meta[k], S * sizeof(uint32_t)));
+  {
+    ScopeMs timer(sim->alloc_ms);
+    const int dev = sim->device;
+    cudaStream_t st = sim->stream;
+    for (int k = 0; k < 2; ++k) {
+      CK(pool_alloc(&sim->d_pbuf[k], S * F_COUNT * sizeof(float), dev, st));
+      CK(pool_alloc(&sim->d_meta[k], S * sizeof(uint32_t), dev, st));
+    }
+    CK(pool_alloc(&sim->d_pic, S * 6 * sizeof(float), dev, st));
+    CK(pool_alloc(&sim->d_key, S * sizeof(uint32_t), dev, st));
+    CK(pool_alloc(&sim->d_rank, S * sizeof(uint32_t), dev, st));
+    CK(pool_alloc(&sim->d_sorted, S * sizeof(uint32_t), dev, st));
+    CK(pool_alloc(&sim->d_active, std::max(n, 1u), dev, st));
   }
-  CK(cudaMalloc(&sim->d_pic, S * 6 * sizeof(float)));
-  CK(cudaMalloc(&sim->d_key, S * sizeof(uint32_t)));
-  CK(cudaMalloc(&sim->d_rank, S * sizeof(uint32_t)));
-  CK(cudaMalloc(&sim->d_sorted, S * sizeof(uint32_t)));
-  CK(cudaMalloc(&sim->d_active, std::max(n, 1u)));
   Params up{};
   up.np = (int)n;
   up.np_stride = (int)S;
@@ -1535,11 +1607,16 @@ pm_status pm_profile_steps(pm_sim* sim, uint32_t nsteps, float* kernel_ms, uint3
   const int K = kernels_per_step(sim->P);
   if ((int)n_kernels < K) return fail(PM_ERR_INVALID, "kernel_ms needs kernels_per_step entries");
   CK(cudaSetDevice(sim->device));
+  // the steps of pm_advance (frame bookkeeping after every step): without it dt would be clipped
+  // to min_dt once the run passes a frame boundary that nothing marks finished
+  pm_status st = sim->sync_ctrl();
+  if (st != PM_OK) return st;
+  const uint32_t af = sim->h_ctrl->auto_frame;
+  if (!af) { sim->h_ctrl->auto_frame = 1; if ((st = sim->push_ctrl()) != PM_OK) return st; }
   std::vector<cudaEvent_t> ev(K + 1);
   for (auto& e : ev) CK(cudaEventCreate(&e));
   std::vector<double> acc(K, 0.0);
   uint32_t done_steps = 0;
-  pm_status st = PM_OK;
   for (uint32_t k = 0; k < nsteps && st == PM_OK; ++k) {
     launch_step(sim->P, sim->bufs(sim->cur), sim->stream, ev.data());
     if (cudaStreamSynchronize(sim->stream) != cudaSuccess) { st = fail(PM_ERR_CUDA, "profiled step failed"); break; }
@@ -1557,6 +1634,11 @@ pm_status pm_profile_steps(pm_sim* sim, uint32_t nsteps, float* kernel_ms, uint3
   }
   for (auto& e : ev) cudaEventDestroy(e);
   for (int i = 0; i < K; ++i) kernel_ms[i] = done_steps ? (float)(acc[i] / done_steps) : 0.f;
+  if (!af) {
+    pm_status s2 = sim->sync_ctrl();
+    if (s2 == PM_OK) { sim->h_ctrl->auto_frame = 0; s2 = sim->push_ctrl(); }
+    if (st == PM_OK) st = s2;
+  }
   return st;
 }
 

@@ -25,7 +25,7 @@ _SCALARS = ("cfl", "cfl_elastic", "flip_ratio", "rho", "E", "nu", "fps", "end_fr
             "sample_log_every")
 _READONLY = ("time", "dt", "step", "Np", "mu", "lambda", "K", "dt_max", "frame_dt", "final_time",
              "n_active", "plastic_count", "grid_nodes", "frame", "kernels_per_step", "regrowths", "regrow_ms",
-             "grid_capacity_nodes")
+             "grid_capacity_nodes", "alloc_ms", "graph_ms")
 _VECTORS = ("gravity", "particle_boundary_min", "particle_boundary_max", "grid_reference_point")
 
 
