@@ -8,8 +8,11 @@
 //
 // Parity pinning: the reference itself cannot be built (Eigen3, OpenVDB, tinyply,
 // tph_poisson and googletest are absent and there is no network), so this restatement is
-// pinned against the reference's own analytic known-answer tests (matter/tests/tests.cpp)
-// and against golden vectors produced by the reference's mixbox library compiled in place.
+// checked against the reference's own known-answer tests (matter/tests/tests.cpp: the curve
+// slide, Coulomb friction on a plate and on the ground object, the bulk modulus, the rotation
+// energy and the Drucker-Prager column collapse; restated in tests/reference_kats.py and run by
+// tests/test_reference_kats.py) and against golden vectors produced by the reference's mixbox
+// library compiled in place.
 //
 // Structure mirrors the reference on purpose so that its CPU cost is representative:
 //   * AoS particle/grid storage, a 4x4x4 precomputed weight stencil per particle
