@@ -784,15 +784,36 @@ def _e2e_breakdown(scene, args, device):
             "readback_bytes": (ox.numel() + ol.numel() + od.numel()) * 4, "total_ms": sum(ms)}
 
 
+def _train_on(scene, args, device):
+    """A surrogate trained on the scene's own samples: args.log_steps plain steps logging about one
+    in `every` Newton solves, then the library's GPU training."""
+    from pigment_mixing_b200 import Simulation, scenes, surrogate
+    npart = len(scene["x"])
+    log = Simulation(device)
+    scenes.apply(scene, log)
+    every = max(1, int(round(npart * args.log_steps / 4e6)))
+    log.set(sample_log_every=every)
+    log.enableSampleLog(6 << 20)
+    log.prepareSimulation()
+    log.advance(args.log_steps)
+    xs, ys = log.samples()
+    log.close()
+    params, hist = surrogate.train(xs, ys, epochs=args.train_epochs, batch=8192, lr=3e-3, seed=0)
+    return params, {"samples": int(len(xs)), "log_every": every, "loss_last_epoch": float(hist[-1])}
+
+
 def _big_point(args, device, params):
     """The 8,388,608-particle scene (four 64^3-cell blocks of four pigments at dx = 1/384): plain and
     surrogate forms, device-timed like the headline, with the surrogate's acceptance and its
-    difference from the plain path after the same steps."""
+    difference from the plain path after the same steps.  The surrogate is trained on this scene's
+    own logged samples (as the 2M leg's is on its scene's)."""
     import torch
     from pigment_mixing_b200 import RETURN_MAP_SURROGATE, Simulation, scenes
     sc = _workload("8m")
     n = len(sc["x"])
     out = {"workload": sc["name"], "particles": n, "steps": args.steps}
+    if params is not None:
+        params, out["surrogate_training"] = _train_on(sc, args, device)
     ref = None
     for form in ("plain", "surrogate"):
         if form == "surrogate" and params is None:

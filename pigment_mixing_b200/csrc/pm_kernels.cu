@@ -53,6 +53,13 @@ __device__ __forceinline__ float bsdN(float u) {
   return 0.f;
 }
 
+// 1: the transfer kernels load the next chunk's (or particle's) sorted index during the current
+// one and prefetch the particle fields it will read into L2 once that index is known.
+#ifndef PM_PREFETCH
+#define PM_PREFETCH 1
+#endif
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 __device__ __forceinline__ void red_add_v4(float4* addr, float a, float b, float c, float d) {
   asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
                : "memory");
@@ -728,11 +735,22 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
       for (int i = threadIdx.x; i < kP2GCh * kTileStride / 4; i += kThreads) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
+#if PM_PREFETCH
+    uint32_t o_next = ps + 32u * warp + lane < pe ? B.sorted[ps + 32u * warp + lane] : 0u;
+#endif
     for (uint32_t c0 = ps + 32u * warp; c0 < pe; c0 += 32u * kWarps) {
       const int n = (int)min(32u, pe - c0);
       int cl = -1;
+#if PM_PREFETCH
+      const uint32_t o_cur = o_next, c1 = c0 + 32u * kWarps;
+      o_next = c1 + lane < pe ? B.sorted[c1 + lane] : 0u;
+#endif
       if (lane < n) {
+#if PM_PREFETCH
+        const uint32_t o = o_cur;
+#else
         const uint32_t o = B.sorted[c0 + lane];
+#endif
         AxisW aw[3];
         float r[3];
 #pragma unroll
@@ -779,6 +797,17 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
         st[7 * 32 + lane] = make_float4(lat[6], 0.f, 0.f, 0.f);
 #endif
       }
+#if PM_PREFETCH
+      if (c1 + lane < pe) {  // the next chunk's fields, while this chunk scatters
+        const float* q = B.pin + o_next;
+#pragma unroll
+        for (int f = F_X; f < F_F; ++f) prefetch_l2(q + (size_t)f * S);
+#pragma unroll
+        for (int f = F_LAT; f < F_EPD; ++f) prefetch_l2(q + (size_t)f * S);
+#pragma unroll
+        for (int f = F_TAU; f < F_COUNT; ++f) prefetch_l2(q + (size_t)f * S);
+      }
+#endif
       // runs of equal cells among the warp's particles
       const int prev = __shfl_up_sync(0xffffffffu, cl, 1);
       uint32_t heads = __ballot_sync(0xffffffffu, lane < n && (lane == 0 || cl != prev));
@@ -1203,12 +1232,23 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
       for (int i = threadIdx.x; i < kTileStride; i += kThreads) m4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
+#if PM_PREFETCH
+    uint32_t o_next = ps + 32u * warp + lane < pe ? B.sorted[ps + 32u * warp + lane] : 0u;
+#endif
     for (uint32_t c0 = ps + 32u * warp; c0 < pe; c0 += 32u * kWarps) {
       const int n = (int)min(32u, pe - c0);
       int cl = -1;
+#if PM_PREFETCH
+      const uint32_t o_cur = o_next, c1 = c0 + 32u * kWarps;
+      o_next = c1 + lane < pe ? B.sorted[c1 + lane] : 0u;
+#endif
       if (lane < n) {
         const uint32_t i = c0 + lane;
+#if PM_PREFETCH
+        const uint32_t o = o_cur;
+#else
         const uint32_t o = B.sorted[i];
+#endif
         float lat[7];
         AxisW aw[3];
 #pragma unroll
@@ -1417,6 +1457,19 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
 #endif
         }
       }
+#if PM_PREFETCH
+      if (c1 + lane < pe) {  // the next chunk's position and latent, while this chunk scatters
+        const float* q = B.pin + o_next;
+#pragma unroll
+        for (int f = F_X; f < F_X + 3; ++f) prefetch_l2(q + (size_t)f * S);
+#pragma unroll
+        for (int f = F_LAT; f < F_LAT + 7; ++f) prefetch_l2(q + (size_t)f * S);
+        if (kFlip || !musl) {
+#pragma unroll
+          for (int f = F_V; f < F_V + 3; ++f) prefetch_l2(q + (size_t)f * S);
+        }
+      }
+#endif
       if (musl) {
         const int prev = __shfl_up_sync(0xffffffffu, cl, 1);
         uint32_t heads = __ballot_sync(0xffffffffu, lane < n && (lane == 0 || cl != prev));
@@ -1967,8 +2020,7 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     po[F_EPV * S + i] = epv;
     po[F_EPP * S + i] = epp;
   };
-  auto particle = [&](const int i) {
-    const uint32_t o = B.sorted[i];
+  auto particle = [&](const int i, const uint32_t o) {
     const uint32_t meta = B.meta_in[o];
     float xp[3];
     AxisW aw[3];
@@ -2098,7 +2150,22 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
       vt[tn] = v;
     }
     __syncthreads();
-    for (int i = (int)ps + threadIdx.x; i < (int)pe; i += blockDim.x) particle(i);
+#if PM_PREFETCH
+    uint32_t o_next = (int)ps + (int)threadIdx.x < (int)pe ? B.sorted[ps + threadIdx.x] : 0u;
+    for (int i = (int)ps + threadIdx.x; i < (int)pe; i += blockDim.x) {
+      const uint32_t o = o_next;
+      const int i2 = i + (int)blockDim.x;
+      o_next = i2 < (int)pe ? B.sorted[i2] : 0u;
+      particle(i, o);
+      if (i2 < (int)pe) {  // the next particle's position and meta word
+        prefetch_l2(B.meta_in + o_next);
+#pragma unroll
+        for (int f = F_X; f < F_X + 3; ++f) prefetch_l2(pi + (size_t)f * S + o_next);
+      }
+    }
+#else
+    for (int i = (int)ps + threadIdx.x; i < (int)pe; i += blockDim.x) particle(i, B.sorted[i]);
+#endif
   }
   // inactive particles sit behind every brick in the sorted order: carried through unchanged
   // (G2P zeroes B, the deformation update zeroes delta_gamma)

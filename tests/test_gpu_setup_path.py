@@ -190,3 +190,27 @@ def test_setup_scene_blobs_builds_the_blob_recipe():
     q = g.getParticles(fields=("x", "active"))
     assert np.isfinite(q.x).all() and q.active.all() and g.errorFlags() == 0
     g.close()
+
+
+def test_simulate_stops_at_max_steps_and_trim_memory_keeps_working():
+    """pm_simulate with a step bound below the run's length reports PM_ERR_STATE after exactly that
+    many steps; pm_trim_memory hands the pool's cached memory back, and simulations created
+    afterwards allocate and step as before."""
+    import ctypes as C
+    from pigment_mixing_b200 import Simulation, scenes
+    from pigment_mixing_b200._lib import PMError, call
+    sc = scenes.two_block_scene(1.0 / 32, (4, 4, 4), seed=8, steps=5)
+    sc["params"]["end_frame"] = 5
+    g = Simulation(0)
+    scenes.apply(sc, g)
+    with pytest.raises(PMError):
+        g.simulate(max_steps=7)
+    assert g.steps_done == 7 and g.frame < 5
+    g.close()
+    call("pm_trim_memory", 0, C.c_uint64(0))
+    g = Simulation(0)
+    scenes.apply(sc, g)
+    steps = g.simulate()
+    assert g.frame == 5 and steps > 7 and g.errorFlags() == 0
+    g.close()
+    call("pm_trim_memory", 0, C.c_uint64(1 << 30))
