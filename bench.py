@@ -851,6 +851,81 @@ def _big_point(args, device, params):
     return out
 
 
+def _active_nodes(sim) -> int:
+    """Grid nodes holding mass after the last step (reads the node masses only)."""
+    import ctypes as C
+    from pigment_mixing_b200._lib import call
+    origin = np.zeros(3)
+    dims = np.zeros(3, np.uint32)
+    up = dims.ctypes.data_as(C.POINTER(C.c_uint32))
+    dp = origin.ctypes.data_as(C.POINTER(C.c_double))
+    call("pm_get_grid", sim._h, dp, up, None, None, None, None, None, None)
+    mass = np.zeros(int(np.prod(dims.astype(np.int64))), np.float32)
+    call("pm_get_grid", sim._h, dp, up, mass.ctypes.data_as(C.POINTER(C.c_float)), None, None, None, None, None)
+    return int((mass > 0).sum())
+
+
+def long_run(args):
+    """The workload's full step count in both return-map forms (the large scene's report): particle-
+    steps/s over the whole run, per-kernel HBM throughput at the end of the run (algorithmic bytes of
+    each transfer kernel over its CUDA-event time), and how far the surrogate form's final latents
+    are from the plain path's: per latent channel, the total variation distance between the two
+    histograms (64 bins over the channel's joint range), the largest per-particle difference and the
+    difference of the mean latent."""
+    import torch
+    from pigment_mixing_b200 import RETURN_MAP_SURROGATE, Simulation, scenes
+    device = 0
+    torch.cuda.set_device(device)
+    sc = _workload(args.workload)
+    n = len(sc["x"])
+    steps = args.long_steps or int(sc["steps"])
+    params, training = _train_on(sc, args, device)
+    peak, peak_kind = _peaks()
+    out = {"metric": "long_run", "workload": sc["name"], "particles": n, "steps": steps, "unit": METRIC,
+           "surrogate_training": training, "peak_gbs": peak, "peak_source": peak_kind}
+    latents = {}
+    for form in ("plain", "surrogate"):
+        s = Simulation(device)
+        scenes.apply(sc, s)
+        if form == "surrogate":
+            s.setSurrogate(params)
+            s.setReturnMap(RETURN_MAP_SURROGATE)
+        s.prepareSimulation()
+        stream = torch.cuda.ExternalStream(s.stream(), device=device)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.advance(steps)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1)
+        latents[form] = s.getParticles(fields=("latent",)).latent
+        nodes = _active_nodes(s)
+        kms = s.profileSteps(3)
+        gbs = {k: (ALGO_BYTES[k][0] * n + ALGO_BYTES[k][1] * nodes) / (kms[k] / 1e3) / 1e9 for k in ALGO_BYTES if k in kms}
+        rm = s.returnMapStats()
+        d = {"value": n * steps / (ms / 1e3), "ms_per_step": ms / steps, "active_nodes_end": nodes,
+             "kernel_ms_end": {k: round(v, 4) for k, v in kms.items()},
+             "kernel_gbs_end": {k: round(v, 1) for k, v in gbs.items()},
+             "kernel_frac_end": {k: round(v / peak, 4) for k, v in gbs.items()}, "error_flags": s.errorFlags()}
+        if form == "surrogate":
+            d["fallback_rate_last_step"] = 1.0 - rm["accepted"] / max(1, rm["queued"])
+            d["speedup_vs_plain"] = d["value"] / out["plain"]["value"]
+        out[form] = d
+        s.close()
+    a, b = latents["plain"].astype(np.float64), latents["surrogate"].astype(np.float64)
+    tv = []
+    for c in range(7):
+        lo, hi = min(a[:, c].min(), b[:, c].min()), max(a[:, c].max(), b[:, c].max())
+        ha, _ = np.histogram(a[:, c], bins=64, range=(lo, hi + 1e-12))
+        hb, _ = np.histogram(b[:, c], bins=64, range=(lo, hi + 1e-12))
+        tv.append(0.5 * float(np.abs(ha / len(a) - hb / len(b)).sum()))
+    out["latent_vs_plain"] = {"histogram_tv_distance_by_channel": tv, "histogram_tv_distance_max": max(tv),
+                              "max_abs": float(np.abs(a - b).max()),
+                              "mean_latent_abs": float(np.abs(a.mean(0) - b.mean(0)).max())}
+    print(json.dumps(out), flush=True)
+
+
 def profile_run(args):
     """A fixed step sequence for profiler captures: `--warm` steps through advance() (graphs),
     `--profile` steps timed kernel by kernel with CUDA events (printed as JSON), then `--plain`
@@ -882,6 +957,10 @@ def main():
     ap.add_argument("--workload", default="2m", choices=["2m", "8m", "32k", "32m", "262k"])
     ap.add_argument("--profile-run", action="store_true",
                     help="no bench line: run the profiler-capture sequence (--warm, --profile, --plain)")
+    ap.add_argument("--long-run", action="store_true",
+                    help="no bench line: the workload's full step count in both forms (run rate, per-kernel "
+                         "HBM GB/s, surrogate latent histogram distance), e.g. --workload 32m --long-run")
+    ap.add_argument("--long-steps", type=int, default=0, help="long run: steps (0 = the workload's own count)")
     ap.add_argument("--warm", type=int, default=10, help="profile run: steps through advance() first")
     ap.add_argument("--profile", type=int, default=3, help="profile run: event-timed steps")
     ap.add_argument("--plain", type=int, default=3, help="profile run: plain step() calls at the end")
@@ -904,6 +983,8 @@ def main():
     args = ap.parse_args()
     if args.profile_run:
         return profile_run(args)
+    if args.long_run:
+        return long_run(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
