@@ -58,6 +58,10 @@ __device__ __forceinline__ float bsdN(float u) {
 #ifndef PM_PREFETCH
 #define PM_PREFETCH 1
 #endif
+// 1: the same for the deformation-update tail's particle loop.
+#ifndef PM_PREFETCH_TAIL
+#define PM_PREFETCH_TAIL 0
+#endif
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 __device__ __forceinline__ void red_add_v4(float4* addr, float a, float b, float c, float d) {
@@ -594,6 +598,14 @@ constexpr int kThreads = 128;  // threads per CTA of the brick kernels
 #ifndef PM_G2P_UNROLL_X
 #define PM_G2P_UNROLL_X 3
 #endif
+// 1: the G2P gather forms its B-spline weights where it uses them (fewer live registers).
+#ifndef PM_G2P_POLYW
+#define PM_G2P_POLYW 1
+#endif
+// 1: the same in the deformation head's velocity-gradient gather.
+#ifndef PM_HEAD_POLYW
+#define PM_HEAD_POLYW 1
+#endif
 // 1: the G2P gather's velocity sums in sum-factorised form (rows, then layers, then the stencil).
 #ifndef PM_G2P_FACTORED
 #define PM_G2P_FACTORED 0
@@ -682,6 +694,17 @@ struct StencilPoly2 {
   __device__ __forceinline__ float2 N(float2 f) const { return fma2(fma2(n2, f, n1), f, n0); }
   __device__ __forceinline__ float2 dN(float2 f) const { return fma2(d1, f, d0); }
 };
+
+// The quadratic B-spline weight of stencil node k (0, 1, 2) and its derivative (times 1/dx) as
+// polynomials of the position f in [0.5, 1.5) inside the base cell (StencilPoly's coefficients),
+// for code that forms weights where it uses them instead of keeping all nine per axis live.
+__device__ __forceinline__ float bs_n(float f, int k) {
+  return k == 0 ? fmaf(fmaf(0.5f, f, -1.5f), f, 1.125f) : (k == 1 ? fmaf(fmaf(-1.f, f, 2.f), f, -0.25f)
+                                                                  : fmaf(fmaf(0.5f, f, -0.5f), f, 0.125f));
+}
+__device__ __forceinline__ float bs_dn(float f, int k, float inv_dx) {
+  return (k == 0 ? f - 1.5f : (k == 1 ? fmaf(-2.f, f, 2.f) : f - 0.5f)) * inv_dx;
+}
 
 size_t p2g_smem_bytes() { return sizeof(float) * kP2GCh * kTileStride + sizeof(float4) * kStageP2G * kThreads; }
 
@@ -1254,6 +1277,9 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
 #pragma unroll
         for (int d = 0; d < 3; ++d) aw[d] = axis_weights(B.pin[(F_X + d) * S + o], P.anchor[d], dx, P.inv_dx);
         cl = local_cell(aw, c, bx, by, bz);
+#if PM_G2P_POLYW
+        const float fpos[3] = {aw[0].r * P.inv_dx, aw[1].r * P.inv_dx, aw[2].r * P.inv_dx};
+#endif
         const int lx = cl >> 4, ly = (cl >> 2) & 3, lz = cl & 3;
         // Ls: the velocity gradient's symmetric part, accumulated directly (xx, yy, zz and the
         // doubled off-diagonals xy, xz, yz): only |0.5 (L + L^T)|_F is used
@@ -1306,17 +1332,30 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
 #pragma unroll kG2PUnrollX
         for (int a = 0; a < 3; ++a) {
           const float oa = (float)(a - 1);
+#if PM_G2P_POLYW
+          // weights formed where they are used, from the position in the base cell
+          const float Na = bs_n(fpos[0], a), dNa = bs_dn(fpos[0], a, P.inv_dx);
+#define PM_NB(k) bs_n(fpos[1], k)
+#define PM_DNB(k) bs_dn(fpos[1], k, P.inv_dx)
+#define PM_NC(k) bs_n(fpos[2], k)
+#define PM_DNC(k) bs_dn(fpos[2], k, P.inv_dx)
+#else
           const float Na = a == 0 ? aw[0].N[0] : (a == 1 ? aw[0].N[1] : aw[0].N[2]);
           const float dNa = a == 0 ? aw[0].dN[0] : (a == 1 ? aw[0].dN[1] : aw[0].dN[2]);
+#define PM_NB(k) aw[1].N[k]
+#define PM_DNB(k) aw[1].dN[k]
+#define PM_NC(k) aw[2].N[k]
+#define PM_DNC(k) aw[2].dN[k]
+#endif
 #pragma unroll
           for (int bb = 0; bb < 3; ++bb) {
-            const float nxy = Na * aw[1].N[bb];
-            const float dnxy = dNa * aw[1].N[bb], ndxy = Na * aw[1].dN[bb];
+            const float nxy = Na * PM_NB(bb);
+            const float dnxy = dNa * PM_NB(bb), ndxy = Na * PM_DNB(bb);
 #pragma unroll
             for (int cz = 0; cz < 3; ++cz) {
               const int tn = ((lx + a) * kTile + (ly + bb)) * kTile + (lz + cz);
-              const float w = nxy * aw[2].N[cz];
-              const float g0 = dnxy * aw[2].N[cz], g1 = ndxy * aw[2].N[cz], g2 = nxy * aw[2].dN[cz];
+              const float w = nxy * PM_NC(cz);
+              const float g0 = dnxy * PM_NC(cz), g1 = ndxy * PM_NC(cz), g2 = nxy * PM_DNC(cz);
               const float4 R0 = tile[tn], R1 = tile[kG2PTileStride + tn], R2 = tile[2 * kG2PTileStride + tn];
               const float gv[3] = {R0.x, R0.y, R0.z};
 #pragma unroll
@@ -1333,6 +1372,10 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
               Ls[3] += gv[0] * g1 + gv[1] * g0;
               Ls[4] += gv[0] * g2 + gv[2] * g0;
               Ls[5] += gv[1] * g2 + gv[2] * g1;
+#undef PM_NB
+#undef PM_DNB
+#undef PM_NC
+#undef PM_DNC
 #endif
               if (use_flip) {
                 const float4 R3 = tile[3 * kG2PTileStride + tn];
@@ -2031,6 +2074,9 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     }
     const int cl = local_cell(aw, c, bx, by, bz);
     const int t0 = ((cl >> 4) * kTile + ((cl >> 2) & 3)) * kTile + (cl & 3);
+#if PM_HEAD_POLYW
+    const float fpos[3] = {aw[0].r * P.inv_dx, aw[1].r * P.inv_dx, aw[2].r * P.inv_dx};
+#endif
     // velocity gradient from the MUSL grid (deformation_update.cpp:26-39)
     float L[9];
 #pragma unroll
@@ -2039,16 +2085,27 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     // per-layer values are picked with selects, not indexed, so they stay in registers
 #pragma unroll kDefgradUnrollX
     for (int a = 0; a < 3; ++a) {
+#if PM_HEAD_POLYW
+      // weights formed where they are used, from the position in the base cell
+      const float Na = bs_n(fpos[0], a), dNa = bs_dn(fpos[0], a, P.inv_dx);
+#define PM_HN(d, k) bs_n(fpos[d], k)
+#define PM_HDN(d, k) bs_dn(fpos[d], k, P.inv_dx)
+#else
       const float Na = a == 0 ? aw[0].N[0] : (a == 1 ? aw[0].N[1] : aw[0].N[2]);
       const float dNa = a == 0 ? aw[0].dN[0] : (a == 1 ? aw[0].dN[1] : aw[0].dN[2]);
+#define PM_HN(d, k) aw[d].N[k]
+#define PM_HDN(d, k) aw[d].dN[k]
+#endif
 #pragma unroll
       for (int bb = 0; bb < 3; ++bb)
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
           const float4 m = vt[t0 + (a * kTile + bb) * kTile + cc];
           const float gv[3] = {m.x, m.y, m.z};
-          const float g[3] = {dNa * aw[1].N[bb] * aw[2].N[cc], Na * aw[1].dN[bb] * aw[2].N[cc],
-                              Na * aw[1].N[bb] * aw[2].dN[cc]};
+          const float g[3] = {dNa * PM_HN(1, bb) * PM_HN(2, cc), Na * PM_HDN(1, bb) * PM_HN(2, cc),
+                              Na * PM_HN(1, bb) * PM_HDN(2, cc)};
+#undef PM_HN
+#undef PM_HDN
 #pragma unroll
           for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -2103,8 +2160,25 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
   };
   if constexpr (kPart == 2) {
     const int nact_sorted = (int)B.cell[c->n_nodes];
+#if PM_PREFETCH_TAIL
+    const int i0 = blk_ * blockDim.x + threadIdx.x;
+    uint32_t o_next = i0 < nact_sorted ? B.sorted[i0] : 0u;
+#endif
     for (int i = blk_ * blockDim.x + threadIdx.x; i < nact_sorted; i += stride) {
+#if PM_PREFETCH_TAIL
+      // the next particle's sorted index now, its F and plastic state into L2 (below)
+      const uint32_t o = o_next;
+      const int i2 = i + stride;
+      o_next = i2 < nact_sorted ? B.sorted[i2] : 0u;
+      if (i2 < nact_sorted) {
+#pragma unroll
+        for (int f = F_F; f < F_F + 9; ++f) prefetch_l2(pi + (size_t)f * S + o_next);
+#pragma unroll
+        for (int f = F_EPD; f < F_DG; ++f) prefetch_l2(pi + (size_t)f * S + o_next);
+      }
+#else
       const uint32_t o = B.sorted[i];
+#endif
       // F_trial = F + dt L F (FP64)
       double L[9], F[9], Ft[9];
 #pragma unroll
