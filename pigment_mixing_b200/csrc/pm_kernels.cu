@@ -606,6 +606,11 @@ constexpr int kThreads = 128;  // threads per CTA of the brick kernels
 #ifndef PM_HEAD_POLYW
 #define PM_HEAD_POLYW 1
 #endif
+// 1: the G2P gather in two passes over the stencil (velocity, APIC and gradient sums, then latent,
+// shear and FLIP sums), so that fewer sums are live at once.
+#ifndef PM_G2P_TWOPASS
+#define PM_G2P_TWOPASS 0
+#endif
 // 1: the G2P gather's velocity sums in sum-factorised form (rows, then layers, then the stencil).
 #ifndef PM_G2P_FACTORED
 #define PM_G2P_FACTORED 0
@@ -1377,11 +1382,12 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
 #undef PM_NC
 #undef PM_DNC
 #endif
+              gl[0] += R0.w * w;
+#if !PM_G2P_TWOPASS
               if (use_flip) {
                 const float4 R3 = tile[3 * kG2PTileStride + tn];
                 fp[0] += R3.x * w; fp[1] += R3.y * w; fp[2] += R3.z * w;
               }
-              gl[0] += R0.w * w;
 #if PM_PACKED
               const float2 w2 = dup2(w);
               g12 = fma2(w2, lo2(R1), g12);
@@ -1392,6 +1398,7 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
               gl[1] += R1.x * w; gl[2] += R1.y * w; gl[3] += R1.z * w; gl[4] += R1.w * w;
               gl[5] += R2.x * w; gl[6] += R2.y * w;
               gs += R2.z * w;
+#endif
 #endif
             }
 #if PM_G2P_FACTORED
@@ -1424,6 +1431,51 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
           Ls[5] += Na * (Sd[2] + SQ[1]);
 #endif
         }
+#if PM_G2P_TWOPASS
+        // second pass over the stencil: latent, shear and the FLIP velocity change, so that these
+        // sums are not live together with the velocity, APIC and gradient sums of the first
+#pragma unroll kG2PUnrollX
+        for (int a = 0; a < 3; ++a) {
+#if PM_G2P_POLYW
+          const float Na = bs_n(fpos[0], a);
+#else
+          const float Na = a == 0 ? aw[0].N[0] : (a == 1 ? aw[0].N[1] : aw[0].N[2]);
+#endif
+#pragma unroll
+          for (int bb = 0; bb < 3; ++bb) {
+#if PM_G2P_POLYW
+            const float nxy = Na * bs_n(fpos[1], bb);
+#else
+            const float nxy = Na * aw[1].N[bb];
+#endif
+#pragma unroll
+            for (int cz = 0; cz < 3; ++cz) {
+              const int tn = ((lx + a) * kTile + (ly + bb)) * kTile + (lz + cz);
+#if PM_G2P_POLYW
+              const float w = nxy * bs_n(fpos[2], cz);
+#else
+              const float w = nxy * aw[2].N[cz];
+#endif
+              const float4 R1 = tile[kG2PTileStride + tn], R2 = tile[2 * kG2PTileStride + tn];
+              if (use_flip) {
+                const float4 R3 = tile[3 * kG2PTileStride + tn];
+                fp[0] += R3.x * w; fp[1] += R3.y * w; fp[2] += R3.z * w;
+              }
+#if PM_PACKED
+              const float2 w2 = dup2(w);
+              g12 = fma2(w2, lo2(R1), g12);
+              g34 = fma2(w2, hi2(R1), g34);
+              g56 = fma2(w2, lo2(R2), g56);
+              gsm = fma2(w2, hi2(R2), gsm);
+#else
+              gl[1] += R1.x * w; gl[2] += R1.y * w; gl[3] += R1.z * w; gl[4] += R1.w * w;
+              gl[5] += R2.x * w; gl[6] += R2.y * w;
+              gs += R2.z * w;
+#endif
+            }
+          }
+        }
+#endif
 #if PM_PACKED
         gl[1] = g12.x; gl[2] = g12.y; gl[3] = g34.x; gl[4] = g34.y; gl[5] = g56.x; gl[6] = g56.y;
         gs = gsm.x;
