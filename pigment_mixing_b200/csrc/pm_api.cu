@@ -151,6 +151,7 @@ struct pm_sim {
   float4* d_grid = nullptr;
   float4* d_gmusl = nullptr;
   uint8_t* d_btouch = nullptr;
+  uint32_t* d_blist = nullptr;  // 4 counts, then the occupied and touched brick lists
 
   Ctrl* d_ctrl = nullptr;
   Ctrl* h_ctrl = nullptr;  // pinned mirror
@@ -302,9 +303,10 @@ void pm_sim::drop_graphs() {
 }
 
 void pm_sim::free_grid() {
-  for (void* p : {(void*)d_cell, (void*)d_scan_part, (void*)d_grid, (void*)d_gmusl, (void*)d_btouch})
+  for (void* p : {(void*)d_cell, (void*)d_scan_part, (void*)d_grid, (void*)d_gmusl, (void*)d_btouch, (void*)d_blist})
     if (p) cudaFreeAsync(p, stream);
   d_cell = nullptr; d_scan_part = nullptr; d_grid = nullptr; d_gmusl = nullptr; d_btouch = nullptr;
+  d_blist = nullptr;
   brick_cap = 0;
 }
 
@@ -327,6 +329,9 @@ struct ScopeMs {
   ~ScopeMs() { acc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
 };
 
+// Scan blocks (4096 cell counters, 64 bricks each) of a grid of the given brick capacity, plus one.
+static size_t scan_blocks_alloc(int bricks) { return ((size_t)bricks * kBrickNodes + 1 + 4095) / 4096 + 1; }
+
 pm_status pm_sim::alloc_grid(int bricks) {
   ScopeMs timer(alloc_ms);
   drop_graphs();
@@ -334,14 +339,17 @@ pm_status pm_sim::alloc_grid(int bricks) {
   const size_t nodes = (size_t)bricks * kBrickNodes;
   if (nodes + 2 > 0x7fffffffULL) return fail(PM_ERR_CAPACITY, "grid capacity exceeds 2^31 nodes");
   CK(pool_alloc(&d_cell, (nodes + 2) * sizeof(uint32_t), device, stream));
-  const size_t scan_blocks = (nodes + 1 + 4095) / 4096 + 1;
-  CK(pool_alloc(&d_scan_part, scan_blocks * sizeof(uint32_t), device, stream));
+  const size_t scan_blocks = scan_blocks_alloc(bricks);
+  // per scan block: the partial sum, the count of occupied bricks, the 64-bit occupancy mask
+  CK(pool_alloc(&d_scan_part, scan_blocks * 4 * sizeof(uint32_t), device, stream));
   CK(pool_alloc(&d_grid, nodes * 4 * sizeof(float4), device, stream));
   CK(pool_alloc(&d_gmusl, nodes * sizeof(float4), device, stream));
   // grid records need no zeroing here: each step zeroes the bricks it touches (k_clear_bricks)
   // and readers see only touched bricks
   CK(pool_alloc(&d_btouch, (size_t)bricks, device, stream));
   CK(cudaMemsetAsync(d_btouch, 0, (size_t)bricks, stream));
+  CK(pool_alloc(&d_blist, (4 + 5 * (size_t)bricks) * sizeof(uint32_t), device, stream));
+  CK(cudaMemsetAsync(d_blist, 0, 4 * sizeof(uint32_t), stream));
   CK(cudaStreamSynchronize(stream));  // the buffers are complete for every stream from here
   brick_cap = bricks;
   return PM_OK;
@@ -359,9 +367,15 @@ Bufs pm_sim::bufs(int parity) const {
   b.sorted = d_sorted;
   b.cell = d_cell;
   b.scan_part = d_scan_part;
+  b.scan_occ = d_scan_part ? d_scan_part + scan_blocks_alloc(brick_cap) : nullptr;
+  b.occ_mask = d_scan_part ? reinterpret_cast<unsigned long long*>(d_scan_part + 2 * scan_blocks_alloc(brick_cap))
+                           : nullptr;
   b.grid = d_grid;
   b.gmusl = d_gmusl;
   b.btouch = d_btouch;
+  b.blist_n = d_blist;
+  b.blist_occ = d_blist ? reinterpret_cast<uint4*>(d_blist + 4) : nullptr;
+  b.blist_touch = d_blist ? d_blist + 4 + 4 * (size_t)brick_cap : nullptr;
   b.ctrl = d_ctrl;
   b.mlp = mlp_dev;
   b.slog = d_slog;

@@ -186,9 +186,18 @@ struct Bufs {
   uint32_t* sorted;       // new position -> read index
   uint32_t* cell;         // node_cap + 2: counts, then exclusive prefix (cell starts)
   uint32_t* scan_part;    // per scan block partial sums
+  uint32_t* scan_occ;     // per scan block (64 bricks): bricks holding particles
+  unsigned long long* occ_mask;  // per scan block: bit j set when brick 64 * block + j holds particles
   float4* grid;           // node_cap * 4 float4
   float4* gmusl;          // node_cap float4
   uint8_t* btouch;        // brick_cap: 1 when a particle's stencil reaches the brick this step
+  // Brick lists of this step: blist_n[0] bricks holding particles, in ascending order (blist_occ,
+  // written by the scan), and blist_n[1] bricks that a particle's stencil reaches (blist_touch,
+  // written by k_clear_bricks).  The transfer kernels walk these instead of the whole box, which
+  // the knife can stretch to many times the bricks the paint fills.
+  uint32_t* blist_n;      // 4 words: counts
+  uint4* blist_occ;       // brick_cap: (brick, first particle, end particle, 0) in sorted order
+  uint32_t* blist_touch;  // brick_cap
   Ctrl* ctrl;
   // learned return map (optional)
   MlpDev mlp;

@@ -177,6 +177,7 @@ __device__ __forceinline__ void d_prologue(const Params& P, const Bufs& B, const
   c->newton_iters = 0;
   c->newton_solves = 0;
   c->sur_accept = 0;
+  B.blist_n[1] = 0u;  // the touched-brick list that k_clear_bricks fills
 }
 __global__ void k_prologue(Params P, Bufs B) { d_prologue(P, B, blockIdx.x, gridDim.x); }
 __global__ void kb_prologue(const SceneDev* __restrict__ sd, const int* __restrict__ off, int ns) {
@@ -349,36 +350,49 @@ __global__ void kb_clear(const SceneDev* __restrict__ sd, const int* __restrict_
 
 // After the scan: a brick is touched this step when one of the bricks b - d, d in {0,1}^3, holds
 // particles (a particle's 3x3x3 stencil spans its own brick and the next one on each axis).
-// One warp per brick: lanes 0..7 test the eight source bricks, then the warp zeroes the brick's
-// 64 accumulated records and MUSL records and stores the flag that k_grid_update reads.  Only
-// touched bricks are ever read by the transfers, so untouched ones are left as they are.
+// A warp takes 32 consecutive bricks, lane j testing brick b0 + j: it stores the touch flags,
+// appends the touched bricks to this step's list (one atomic per warp) and then zeroes the
+// accumulated and MUSL records of each touched brick in turn.  Consecutive groups of 32 bricks go
+// to different CTAs, so that a small box still spreads its zeroing over the SMs.  Only touched
+// bricks are ever read by the transfers, so untouched ones are left as they are.
 __device__ __forceinline__ void d_clear_bricks(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
   if (c->halt || c->idle) return;
   const int nbr = c->n_bricks, lane = threadIdx.x & 31;
-  const int warps = nblk_ * (blockDim.x >> 5);
+  const int wpc = blockDim.x >> 5, warps = nblk_ * wpc;
+  const size_t nyz = (size_t)c->nb[1] * c->nb[2], nz = (size_t)c->nb[2];
   const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (int b = blk_ * (blockDim.x >> 5) + (threadIdx.x >> 5); b < nbr; b += warps) {
-    bool occ = false;
-    if (lane < 8) {
+  for (int b0 = ((threadIdx.x >> 5) * nblk_ + blk_) * 32; b0 < nbr; b0 += warps * 32) {
+    const int b = b0 + lane;
+    bool touched = false;
+    if (b < nbr) {
       int bx, by, bz;
       brick_coords(b, c, bx, by, bz);
-      const int sx = bx - (lane >> 2), sy = by - ((lane >> 1) & 1), sz = bz - (lane & 1);
-      if (sx >= 0 && sy >= 0 && sz >= 0) {
-        const size_t sb = ((size_t)sx * c->nb[1] + sy) * c->nb[2] + sz;
-        occ = B.cell[sb * kBrickNodes] != B.cell[(sb + 1) * kBrickNodes];
-      }
-    }
-    const bool touched = __ballot_sync(0xffffffffu, occ) != 0u;
-    if (lane == 0) B.btouch[b] = touched ? 1 : 0;
-    if (!touched) continue;
-    float4* rec = B.grid + (size_t)b * kBrickNodes * 4;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) rec[k * 32 + lane] = z;
-    if (P.use_musl) {
-      float4* m = B.gmusl + (size_t)b * kBrickNodes;
-      m[lane] = z;
-      m[32 + lane] = z;
+      for (int k = 0; k < 8; ++k) {
+        const int sx = bx - (k >> 2), sy = by - ((k >> 1) & 1), sz = bz - (k & 1);
+        if (sx >= 0 && sy >= 0 && sz >= 0) {
+          const size_t sb = (size_t)sx * nyz + (size_t)sy * nz + (size_t)sz;
+          touched = touched || (B.cell[sb * kBrickNodes] != B.cell[(sb + 1) * kBrickNodes]);
+        }
+      }
+      B.btouch[b] = touched ? 1 : 0;
+    }
+    const uint32_t mt = __ballot_sync(0xffffffffu, touched);
+    uint32_t base = 0u;
+    if (lane == 0 && mt) base = atomicAdd(&B.blist_n[1], (uint32_t)__popc(mt));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (touched) B.blist_touch[base + __popc(mt & ((1u << lane) - 1u))] = (uint32_t)b;
+    for (uint32_t m = mt; m; m &= m - 1u) {
+      const size_t tb = (size_t)(b0 + __ffs(m) - 1);
+      float4* rec = B.grid + tb * kBrickNodes * 4;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) rec[k * 32 + lane] = z;
+      if (P.use_musl) {
+        float4* mm = B.gmusl + tb * kBrickNodes;
+        mm[lane] = z;
+        mm[32 + lane] = z;
+      }
     }
   }
 }
@@ -479,6 +493,9 @@ __device__ __forceinline__ void d_scan_local(const Params& P, const Bufs& B, con
   if (c->halt || c->idle) return;
   const int n = c->n_nodes + 1;
   __shared__ uint32_t ws[32];
+  __shared__ uint32_t occ2[kScanThreads / 32];  // per warp: its two bricks' occupancy bits
+  static_assert(kScanBlock == 64 * kBrickNodes && kBrickNodes == 16 * kScanPer, "a scan block is 64 bricks");
+  const int lane = threadIdx.x & 31;
   // grid-stride over the 4096-entry scan blocks of this step's box (the launch is sized for a
   // typical box, not for the grid capacity)
   for (int sb = blk_; sb * kScanBlock < n; sb += nblk_) {
@@ -488,7 +505,10 @@ __device__ __forceinline__ void d_scan_local(const Params& P, const Bufs& B, con
     const int i0 = b0 + threadIdx.x * kScanPer;
 #pragma unroll
     for (int k = 0; k < kScanPer; ++k) { v[k] = (i0 + k < n) ? B.cell[i0 + k] : 0u; tsum += v[k]; }
-    uint32_t incl = block_incl_scan(tsum, ws);
+    // 16 threads hold the 64 counters of one brick: warp w covers bricks 2w and 2w + 1 of the block
+    const uint32_t nz = __ballot_sync(0xffffffffu, tsum != 0u);
+    if (lane == 0) occ2[threadIdx.x >> 5] = ((nz & 0xffffu) ? 1u : 0u) | ((nz >> 16) ? 2u : 0u);
+    uint32_t incl = block_incl_scan(tsum, ws);  // its barriers publish occ2
     uint32_t run = incl - tsum;
 #pragma unroll
     for (int k = 0; k < kScanPer; ++k) {
@@ -496,7 +516,17 @@ __device__ __forceinline__ void d_scan_local(const Params& P, const Bufs& B, con
       run += v[k];
     }
     if (threadIdx.x == kScanThreads - 1) B.scan_part[sb] = incl;
-    __syncthreads();  // ws is reused by the next block's scan
+    if (threadIdx.x == 0) {
+      // occupied bricks of this block; the inactive-particle counter behind the last brick
+      // (entry n_nodes) belongs to no brick
+      unsigned long long m = 0ull;
+      for (int w = 0; w < kScanThreads / 32; ++w) m |= (unsigned long long)occ2[w] << (2 * w);
+      const int first = sb * (kScanBlock / kBrickNodes), valid = c->n_bricks - first;
+      if (valid < 64) m &= valid > 0 ? (1ull << valid) - 1ull : 0ull;
+      B.occ_mask[sb] = m;
+      B.scan_occ[sb] = (uint32_t)__popcll(m);
+    }
+    __syncthreads();  // ws and occ2 are reused by the next block's scan
   }
 }
 __global__ void __launch_bounds__(kScanThreads) k_scan_local(Params P, Bufs B) { d_scan_local(P, B, blockIdx.x, gridDim.x); }
@@ -537,18 +567,36 @@ __device__ __forceinline__ void d_scan_add(const Params& P, const Bufs& B, const
   const int n = c->n_nodes + 1;
   const int nb = (n + kScanBlock - 1) / kScanBlock;
   __shared__ uint32_t ws[33];
-  uint32_t off = 0;  // sum of scan_part[0, upto)
+  uint32_t off = 0, off_occ = 0;  // sums of scan_part and scan_occ over [0, upto)
   int upto = 0;
   for (int sb = blk_; sb < nb; sb += nblk_) {
     off += block_range_sum(B.scan_part, upto, sb, ws);
+    off_occ += block_range_sum(B.scan_occ, upto, sb, ws);
     upto = sb;
+    // this block's occupied bricks with their particle ranges, at their place in the ascending list
+    // of occupied bricks: a brick starts at its first counter's block-local prefix plus the block's
+    // offset and ends where the next brick starts (the block total for the block's last brick)
+    if (threadIdx.x < 64) {
+      const unsigned long long m = B.occ_mask[sb];
+      if ((m >> threadIdx.x) & 1ull) {
+        const uint32_t bi = (uint32_t)(sb * (kScanBlock / kBrickNodes) + threadIdx.x);
+        const uint32_t ps = B.cell[(size_t)bi * kBrickNodes] + off;
+        const uint32_t pe = (threadIdx.x < 63 ? B.cell[(size_t)(bi + 1) * kBrickNodes] : B.scan_part[sb]) + off;
+        B.blist_occ[off_occ + (uint32_t)__popcll(m & ((1ull << threadIdx.x) - 1ull))] = make_uint4(bi, ps, pe, 0u);
+      }
+    }
     if (sb == 0) continue;  // block 0 needs no offset
+    __syncthreads();  // the block-local prefixes above are read before they are offset
     const int b0 = sb * kScanBlock;
     for (int i = b0 + threadIdx.x; i < min(b0 + kScanBlock, n); i += kScanThreads) B.cell[i] += off;
   }
   if (blk_ == 0) {
     const uint32_t total = block_range_sum(B.scan_part, 0, nb, ws);
-    if (threadIdx.x == 0) B.cell[n] = total;  // = np
+    const uint32_t occupied = block_range_sum(B.scan_occ, 0, nb, ws);
+    if (threadIdx.x == 0) {
+      B.cell[n] = total;  // = np
+      B.blist_n[0] = occupied;
+    }
   }
 }
 __global__ void __launch_bounds__(kScanThreads) k_scan_add(Params P, Bufs B) { d_scan_add(P, B, blockIdx.x, gridDim.x); }
@@ -626,7 +674,7 @@ constexpr int kDefgradUnrollX = PM_DEFGRAD_UNROLL_X;
 #define PM_SCATTER_UNROLL 1
 #endif
 #ifndef PM_P2G_MINB
-#define PM_P2G_MINB 0
+#define PM_P2G_MINB 6
 #endif
 constexpr int kScatterUnroll = PM_SCATTER_UNROLL;
 constexpr int kWarps = kThreads / 32;
@@ -752,10 +800,21 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
   const StencilPoly2 pxy(px, py);
   const float2 fa2 = dup2(fa), fb2 = dup2(fb), fc2 = dup2(fc);
 #endif
-  const int nbr = c->n_bricks;
-  for (int b = blk_; b < nbr; b += nblk_) {
-    const uint32_t ps = B.cell[(size_t)b * kBrickNodes], pe = B.cell[(size_t)(b + 1) * kBrickNodes];
-    if (ps == pe) continue;
+#ifndef PM_P2G_CHUNKED
+#define PM_P2G_CHUNKED 0
+#endif
+#if PM_P2G_CHUNKED
+  // each CTA takes a contiguous run of the occupied bricks
+  const int per_cta = ((int)B.blist_n[0] + nblk_ - 1) / nblk_;
+  const int ib_end = min((int)B.blist_n[0], (blk_ + 1) * per_cta);
+  for (int ib = blk_ * per_cta; ib < ib_end; ++ib) {
+#else
+  // the list length is re-read per brick (one L1 hit) rather than held across the scatter
+  for (int ib = blk_; ib < (int)B.blist_n[0]; ib += nblk_) {
+#endif
+    const uint4 be = B.blist_occ[ib];
+    const int b = (int)be.x;
+    const uint32_t ps = be.y, pe = be.z;
     int bx, by, bz;
     brick_coords(b, c, bx, by, bz);
     {
@@ -1133,14 +1192,14 @@ __device__ void boundary_collision(const Ctrl* c, float dtf, float dx, float Xi_
 __device__ __forceinline__ void d_grid_update(const Params& P, const Bufs& B, const int blk_, const int nblk_) {
   const Ctrl* c = B.ctrl;
   if (c->halt || c->idle) return;
-  const int nn = c->n_nodes;
+  const int nt = (int)B.blist_n[1] * kBrickNodes;  // nodes of the bricks a stencil reaches
   const float dtf = (float)c->dt;
   const float dtv = dtf * P.particle_volume;
   const float dtg[3] = {dtf * P.gravity[0], dtf * P.gravity[1], dtf * P.gravity[2]};
   const int stride = nblk_ * blockDim.x;
   uint32_t err = 0;
-  for (int n = blk_ * blockDim.x + threadIdx.x; n < nn; n += stride) {
-    if (!B.btouch[n >> 6]) continue;  // no particle stencil reaches this brick: record is stale
+  for (int t = blk_ * blockDim.x + threadIdx.x; t < nt; t += stride) {
+    const int n = (int)B.blist_touch[t >> 6] * kBrickNodes + (t & 63);
     float4* rec = B.grid + (size_t)n * 4;
     float4 r0 = rec[0];
     if (!(r0.x > 0.f)) continue;
@@ -1243,10 +1302,11 @@ __device__ __forceinline__ void d_g2p_musl(const Params& P, const Bufs& B, const
     }
   }
   const float dyn = P.D_max * time_factor;
-  const int nbr = c->n_bricks;
-  for (int b = blk_; b < nbr; b += nblk_) {
-    const uint32_t ps = B.cell[(size_t)b * kBrickNodes], pe = B.cell[(size_t)(b + 1) * kBrickNodes];
-    if (ps == pe) continue;
+  const int nbr = (int)B.blist_n[0];
+  for (int ib = blk_; ib < nbr; ib += nblk_) {
+    const uint4 be = B.blist_occ[ib];
+    const int b = (int)be.x;
+    const uint32_t ps = be.y, pe = be.z;
     int bx, by, bz;
     brick_coords(b, c, bx, by, bz);
     for (int i = threadIdx.x; i < kTileNodes * 4; i += kThreads) {
@@ -2254,10 +2314,11 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
       tail(i, o, Ft);
     }
   }
-  const int nbr = kPart == 2 ? 0 : c->n_bricks;
-  for (int b = blk_; b < nbr; b += nblk_) {
-    const uint32_t ps = B.cell[(size_t)b * kBrickNodes], pe = B.cell[(size_t)(b + 1) * kBrickNodes];
-    if (ps == pe) continue;
+  const int nbr = kPart == 2 ? 0 : (int)B.blist_n[0];
+  for (int ib = blk_; ib < nbr; ib += nblk_) {
+    const uint4 be = B.blist_occ[ib];
+    const int b = (int)be.x;
+    const uint32_t ps = be.y, pe = be.z;
     brick_coords(b, c, bx, by, bz);
     __syncthreads();  // the previous brick's readers are done with the tile
     for (int tn = threadIdx.x; tn < kTileNodes; tn += blockDim.x) {
