@@ -386,11 +386,11 @@ PM_API pm_status pm_batch_profile(pm_batch* batch, uint32_t rounds, float* kerne
  * All n particles are treated as active (no active mask, unlike p2g.cpp:22).
  * Scratch is one fixed 8 MiB __device__ array inside the library (held by every GPU that loads
  * it until exit): at most 131072 particles and 131072 nodes per call, PM_ERR_CAPACITY beyond.
- * The first call on a device looks up that array's device address, so make it before any stream
- * capture.  All calls share the array: calls whose work overlaps on the GPU race.  Work is queued
- * on `stream` (NULL = default stream).  When `outside` is not NULL the call synchronises `stream`
+ * The first call on a device looks up that array's device address (a synchronous runtime query).
+ * All calls share the array: calls whose work overlaps on the GPU race.  Work is queued on
+ * `stream` (NULL = default stream).  When `outside` is not NULL the call synchronises `stream`
  * and stores the number of particles skipped because their stencil left the box or a coordinate
- * was not finite; the stream must then not be in capture mode. */
+ * was not finite. */
 PM_API pm_status pm_p2g_noalloc(const float* x, const float* v, const float* B, const float* latent,
                                 const float* diffusion, uint32_t n, double particle_mass, double dx,
                                 const double origin[3], const int32_t dims[3], float* node_mass,

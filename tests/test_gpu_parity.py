@@ -272,6 +272,39 @@ def test_async_readback_matches_sync_readback(small_scene):
     assert not np.array_equal(now.x, ref.x)
 
 
+def test_sparse_box_with_outliers_matches_oracle():
+    """Four particles far from the paint stretch the grid box to dozens of times the bricks that hold
+    particles, as the knife's splashes do: the occupied- and touched-brick lists must still reach
+    every brick, so after one step the grid holds the oracle's nodes with the oracle's values, and
+    after ten steps the particles match."""
+    from pigment_mixing_b200 import scenes
+    sc = scenes.two_block_scene(1.0 / 32, (4, 4, 4), seed=11, steps=10)
+    far = np.float32([[0.05, 0.9, 0.05], [0.95, 0.9, 0.95], [0.05, 0.6, 0.95], [0.95, 0.02, 0.05]])
+    sc["x"] = np.concatenate([sc["x"], far]).astype(np.float32)
+    sc["latent"] = np.concatenate([sc["latent"], sc["latent"][:4]]).astype(np.float32)
+    g, o = _pair(sc)
+    g.advance(1)
+    o.advance(1)
+    dx = sc["params"]["dx"]
+    gg, og = g.grid(), o.grid()
+    box_bricks = int(np.prod(gg["dims"])) // 64
+    mg, mo = _grid_maps(gg, dx, "mass"), _grid_maps(og, dx, "mass")
+    assert set(mg) == set(mo)
+    assert box_bricks > 20 * (len(mo) // 64 + 1)  # the box is mostly empty bricks
+    for kg, ko in (("mass", "mass"), ("v_update", "v_update"), ("latent", "latent")):
+        a, b = _grid_maps(gg, dx, kg), _grid_maps(og, dx, ko)
+        scale = max(1.0, max(np.abs(v).max() for v in b.values()))
+        assert max(np.abs(a[k] - b[k]).max() for k in b) <= 1e-6 * scale, kg
+    g.advance(9)
+    o.advance(9)
+    pg = g.getParticles(fields=("x", "latent", "active"))
+    po = o.particles_f64()
+    assert np.array_equal(pg.active, po["active"])
+    assert np.abs(pg.x - po["x"]).max() <= 1e-5
+    assert np.abs(pg.latent - po["latent"]).max() <= 1e-5
+    assert g.errorFlags() == 0
+
+
 @pytest.mark.parametrize("count", [1, 7, 33, 1000])
 def test_ragged_particle_counts_match_oracle(count):
     """Particle counts that fill no warp, CTA or brick evenly (a single particle, 7, 33, 1000 drawn
