@@ -728,6 +728,7 @@ def _e2e(scene, args, device, dist, ws):
     sim.waitReadback()
     marks.append(time.perf_counter())
     el = time.perf_counter() - t0
+    alloc_ms, graph_ms = float(sim.alloc_ms), float(sim.graph_ms)
     sim.close()
     ms = [round(1e3 * (marks[i + 1] - marks[i]), 2) for i in range(len(marks) - 1)]
     el_max = _max_over_ranks(dist, el, device)
@@ -738,7 +739,8 @@ def _e2e(scene, args, device, dist, ws):
             "includes": "creation, upload, prepare, K steps, per-frame x/latent/diffusion readback (overlapped "
                         "with the following steps), final readback; after one untimed pass",
             "host_ms": {"create_upload": ms[0], "setup_prepare": ms[1], "advance_chunks": ms[2:-1],
-                        "final_readback": ms[-1]}}
+                        "final_readback": ms[-1], "of_which_alloc": round(alloc_ms, 2),
+                        "of_which_graph_build": round(graph_ms, 2)}}
 
 
 def _e2e_breakdown(scene, args, device):

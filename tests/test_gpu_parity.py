@@ -299,7 +299,7 @@ def test_sparse_box_with_outliers_matches_oracle():
     o.advance(9)
     pg = g.getParticles(fields=("x", "latent", "active"))
     po = o.particles_f64()
-    assert np.array_equal(pg.active, po["active"])
+    assert np.array_equal(pg.active, o.particles()["active"])
     assert np.abs(pg.x - po["x"]).max() <= 1e-5
     assert np.abs(pg.latent - po["latent"]).max() <= 1e-5
     assert g.errorFlags() == 0
