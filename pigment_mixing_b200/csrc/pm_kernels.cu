@@ -69,7 +69,13 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
 }
+// 16 bytes, or 16 zero bytes when !valid (no global read then; gmem must still be a valid address)
+__device__ __forceinline__ void cp_async16_zfill(void* smem, const void* gmem, bool valid) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(valid ? 16 : 0) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ void red_add_v4(float4* addr, float a, float b, float c, float d) {
@@ -662,6 +668,13 @@ constexpr int kThreads = 128;  // threads per CTA of the brick kernels
 #ifndef PM_HEAD_POLYW
 #define PM_HEAD_POLYW 1
 #endif
+// 1: the deformation head loads the next brick's velocity tile and each thread's next particle
+// (meta word, position, pic velocity, G2P velocity) with cp.async into double-buffered shared
+// slots while the current brick and particle are processed.  Measured on the 2M scene: 88, 90,
+// 92, 96 us at steps 1, 20, 100, 500 against 90, 93, 93, 100 us with L2 prefetches.
+#ifndef PM_HEAD_ASYNC
+#define PM_HEAD_ASYNC 1
+#endif
 // 1: the G2P gather in two passes over the stencil (velocity, APIC and gradient sums, then latent,
 // shear and FLIP sums), so that fewer sums are live at once.
 #ifndef PM_G2P_TWOPASS
@@ -808,18 +821,9 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
   const StencilPoly2 pxy(px, py);
   const float2 fa2 = dup2(fa), fb2 = dup2(fb), fc2 = dup2(fc);
 #endif
-#ifndef PM_P2G_CHUNKED
-#define PM_P2G_CHUNKED 0
-#endif
-#if PM_P2G_CHUNKED
-  // each CTA takes a contiguous run of the occupied bricks
-  const int per_cta = ((int)B.blist_n[0] + nblk_ - 1) / nblk_;
-  const int ib_end = min((int)B.blist_n[0], (blk_ + 1) * per_cta);
-  for (int ib = blk_ * per_cta; ib < ib_end; ++ib) {
-#else
-  // the list length is re-read per brick (one L1 hit) rather than held across the scatter
+  // the list length is re-read per brick (one L1 hit) rather than held across the scatter; CTAs take
+  // every nblk_-th brick (contiguous runs of bricks per CTA measured slower: 330 against 291 us)
   for (int ib = blk_; ib < (int)B.blist_n[0]; ib += nblk_) {
-#endif
     const uint4 be = B.blist_occ[ib];
     const int b = (int)be.x;
     const uint32_t ps = be.y, pe = be.z;
@@ -2200,7 +2204,16 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
   const float fr = P.flip_ratio;
   // grid velocities of the brick's 6x6x6 stencil tile: the MUSL velocity (normalised once per
   // node here) or, in USL mode, the updated grid velocity
+#if PM_HEAD_ASYNC
+  __shared__ float4 vt2[2][kTileNodes];
+  // per thread, two slots of its particle's staged words: meta, x (3), pic (3), v (3)
+  constexpr int kHS = 10;
+  __shared__ float hs[2][kHS][kThreads];
+  const float4* vt = vt2[0];
+  int hslot = 0;
+#else
   __shared__ float4 vt[kTileNodes];
+#endif
   int bx = 0, by = 0, bz = 0;
   float* po = B.pout;
   const float* pi = B.pin;
@@ -2238,12 +2251,20 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     po[F_EPP * S + i] = epp;
   };
   auto particle = [&](const int i, const uint32_t o) {
+#if PM_HEAD_ASYNC
+    const uint32_t meta = __float_as_uint(hs[hslot][0][threadIdx.x]);
+#else
     const uint32_t meta = B.meta_in[o];
+#endif
     float xp[3];
     AxisW aw[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
+#if PM_HEAD_ASYNC
+      xp[d] = hs[hslot][1 + d][threadIdx.x];
+#else
       xp[d] = pi[(F_X + d) * S + o];
+#endif
       aw[d] = axis_weights(xp[d], P.anchor[d], dx, P.inv_dx);
     }
     const int cl = local_cell(aw, c, bx, by, bz);
@@ -2289,8 +2310,13 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     // position update (position_update.cpp:6-91); done before the SVD so that its values are not
     // live across it
     float pic[3], v[3];
+#if PM_HEAD_ASYNC
+#pragma unroll
+    for (int r = 0; r < 3; ++r) { pic[r] = hs[hslot][4 + r][threadIdx.x]; v[r] = hs[hslot][7 + r][threadIdx.x]; }
+#else
 #pragma unroll
     for (int r = 0; r < 3; ++r) { pic[r] = B.pic[r * S + i]; v[r] = po[(F_V + r) * S + i]; }
+#endif
     if (!P.use_musl) {
       for (int r = 0; r < 3; ++r) {
         const float fl = B.pic[(3 + r) * S + i];
@@ -2377,6 +2403,65 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     }
   }
   const int nbr = kPart == 2 ? 0 : (int)B.blist_n[0];
+#if PM_HEAD_ASYNC
+  // the velocity tile of brick list entry ib_ into tile slot `slot`, normalised after arrival
+  auto issue_tile = [&](const int ib_, const int slot) {
+    int qx, qy, qz;
+    brick_coords((int)B.blist_occ[ib_].x, c, qx, qy, qz);
+    for (int tn = threadIdx.x; tn < kTileNodes; tn += blockDim.x) {
+      const int node = tile_to_node(tn, qx, qy, qz, c);
+      const float4* src = P.use_musl ? B.gmusl + (node >= 0 ? node : 0) : B.grid + (size_t)(node >= 0 ? node : 0) * 4;
+      cp_async16_zfill(&vt2[slot][tn], src, node >= 0);
+    }
+  };
+  // particle i's staged words (read index o) into particle slot `slot`
+  auto issue_particle = [&](const int i, const uint32_t o, const int slot) {
+    cp_async4(&hs[slot][0][threadIdx.x], B.meta_in + o);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) cp_async4(&hs[slot][1 + d][threadIdx.x], pi + (size_t)(F_X + d) * S + o);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) cp_async4(&hs[slot][4 + r][threadIdx.x], B.pic + (size_t)r * S + i);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) cp_async4(&hs[slot][7 + r][threadIdx.x], po + (size_t)(F_V + r) * S + i);
+  };
+  if (blk_ < nbr) issue_tile(blk_, 0);
+  cp_async_commit();
+  int tslot = 0;
+  for (int ib = blk_; ib < nbr; ib += nblk_, tslot ^= 1) {
+    const uint4 be = B.blist_occ[ib];
+    const int b = (int)be.x;
+    const uint32_t ps = be.y, pe = be.z;
+    brick_coords(b, c, bx, by, bz);
+    __syncthreads();  // the brick before the previous one is done with the other tile slot
+    if (ib + nblk_ < nbr) issue_tile(ib + nblk_, tslot ^ 1);
+    cp_async_commit();
+    cp_async_wait_1();  // this brick's tile (all but the group just committed)
+    __syncthreads();
+    vt = vt2[tslot];
+    if (P.use_musl) {
+      for (int tn = threadIdx.x; tn < kTileNodes; tn += blockDim.x) {
+        const float4 m = vt2[tslot][tn];
+        const float inv = m.w > 0.f ? 1.f / m.w : 0.f;
+        vt2[tslot][tn] = make_float4(m.x * inv, m.y * inv, m.z * inv, 0.f);
+      }
+    }
+    __syncthreads();
+    {
+      int i = (int)ps + (int)threadIdx.x;
+      if (i < (int)pe) issue_particle(i, B.sorted[i], hslot ^ 1);
+      cp_async_commit();
+      for (; i < (int)pe; i += blockDim.x) {
+        hslot ^= 1;  // the slot the copies above went to
+        const uint32_t o = B.sorted[i];
+        const int i2 = i + (int)blockDim.x;
+        if (i2 < (int)pe) issue_particle(i2, B.sorted[i2], hslot ^ 1);
+        cp_async_commit();
+        cp_async_wait_1();  // this particle's words
+        particle(i, o);
+      }
+    }
+  }
+#else
   for (int ib = blk_; ib < nbr; ib += nblk_) {
     const uint4 be = B.blist_occ[ib];
     const int b = (int)be.x;
@@ -2416,6 +2501,7 @@ __device__ __forceinline__ void d_defgrad(const Params& P, const Bufs& B, const 
     for (int i = (int)ps + threadIdx.x; i < (int)pe; i += blockDim.x) particle(i, B.sorted[i]);
 #endif
   }
+#endif
   // inactive particles sit behind every brick in the sorted order: carried through unchanged
   // (G2P zeroes B, the deformation update zeroes delta_gamma)
   for (int i = (int)B.cell[c->n_nodes] + blk_ * blockDim.x + threadIdx.x; kPart != 2 && i < np; i += stride) {
