@@ -104,3 +104,49 @@ def test_vmvisc_projection_is_consistent(oracle_mod):
         q = 2 * prm["q_prefac"] * mu * np.linalg.norm(dev)
         target = prm["q_max"] * (1 + prm["perzyna_visc"] * dg[i]) ** prm["perzyna_exp"]
         assert q == pytest.approx(target, rel=2e-3, abs=0.05)
+
+
+def test_dpvisc_projection_is_consistent(oracle_mod):
+    """plasticity.cpp:240-340 (Pradhana's shift off): after projection every plastic particle off
+    the apex sits on the Perzyna-scaled Drucker-Prager surface, q = (M p + q_cohesion)(1 + eta
+    delta_gamma) with p = -K tr(h) and q = 2 q_prefac mu |dev h| of its final F (h the log
+    singular values); apex particles have q = 0 = M p_tip + q_cohesion.  Observed: 4e-5 relative."""
+    from pigment_mixing_b200 import scenes
+    sc = scenes.two_block_scene(1.0 / 32, (8, 8, 4), seed=1, steps=20, material="dpvisc")
+    sc["params"]["use_pradhana"] = 0
+    o = oracle_mod.OracleSim(64)
+    o.set(n_threads=4)
+    scenes.apply(sc, o)
+    o.prepare()
+    o.advance(15)
+    p = o.particles()
+    prm = sc["params"]
+    K, emu = o.get("K"), 2 * prm["q_prefac"] * o.get("mu")
+    dg = p["plastic"][:, 3].astype(np.float64)
+    idx = np.nonzero(dg > 0)[0]
+    assert len(idx) > len(dg) // 4
+    for i in idx:
+        h = np.log(np.linalg.svd(p["F"][i].astype(np.float64), compute_uv=False))
+        q = emu * np.linalg.norm(h - h.mean())
+        target = (prm["M"] * (-K * h.sum()) + prm["q_cohesion"]) * (1 + prm["perzyna_visc"] * dg[i])
+        assert q == pytest.approx(target, rel=1e-3, abs=0.05)
+
+
+def test_float_oracle_tracks_double_oracle(oracle_mod):
+    """The float restatement (the reference's T = float) against the FP64 oracle over 20 steps of the
+    VMVisc scene: the precision split costs no more than FP32 rounding.  Observed: positions 5e-7,
+    velocities 8e-6 (|v| up to 0.77), latents 4e-6."""
+    from pigment_mixing_b200 import scenes
+    sc = scenes.two_block_scene(1.0 / 32, (8, 8, 4), seed=1, steps=20, material="vmvisc")
+    out = {}
+    for prec in (32, 64):
+        o = oracle_mod.OracleSim(prec)
+        o.set(n_threads=4)
+        scenes.apply(sc, o)
+        o.prepare()
+        o.advance(20)
+        out[prec] = o.particles_f64()
+    a, b = out[32], out[64]
+    assert np.abs(a["x"] - b["x"]).max() <= 1e-5
+    assert np.abs(a["v"] - b["v"]).max() <= 1e-4 * max(1.0, np.abs(b["v"]).max())
+    assert np.abs(a["latent"] - b["latent"]).max() <= 1e-4
