@@ -84,9 +84,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // before it reads anything (griddepcontrol.wait).  PM_PDL 2 leaves the trigger implicit (the
 // previous kernel's completion); PM_PDL 1 also triggers at every CTA's start
 // (launch_dependents), so that the next kernel's CTAs take SMs as the previous kernel's last CTAs
-// free them.  Measured on the 2M scene (graph-timed steps 5-105): 0.929-0.931 ms per step with
-// PM_PDL 2, 0.931-0.936 without, 1.016-1.019 with PM_PDL 1.  Launched without the attribute
-// (batches, single launches) the instructions return at once.
+// free them.  Measured on the 2M scene (graph-timed steps 5-105, three runs each): 0.929-0.931 ms
+// per step with PM_PDL 2, 0.931-0.936 without (the bench's headline measured 0.935 ms both ways,
+// so the gain is within its run-to-run spread), 1.016-1.019 with PM_PDL 1.  Launched without the
+// attribute (batches, single launches) the instructions return at once.
 #ifndef PM_PDL
 #define PM_PDL 2
 #endif
