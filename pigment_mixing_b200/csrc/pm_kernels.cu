@@ -862,6 +862,8 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
     int bx, by, bz;
     brick_coords(b, c, bx, by, bz);
     {
+      // the tile is zeroed before every brick (zeroing each node in the flush instead, which
+      // saves this barrier, measured 0.937 against 0.936 ms per step)
       float4* t4 = reinterpret_cast<float4*>(tile);  // kP2GCh * kTileStride is a multiple of 4
       for (int i = threadIdx.x; i < kP2GCh * kTileStride / 4; i += kThreads) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
@@ -1026,14 +1028,14 @@ __device__ __forceinline__ void d_p2g(const Params& P, const Bufs& B, const int 
     for (int tn = threadIdx.x; tn < kTileNodes; tn += kThreads) {
       const float* t = tile + tile_pad(tn);
       const float m = t[0];
-      if (m == 0.f) continue;
-      const int node = tile_to_node(tn, bx, by, bz, c);
-      if (node < 0) continue;
-      float4* rec = B.grid + (size_t)node * 4;
-      red_add_v4(rec + 0, m, t[1 * kTileStride], t[2 * kTileStride], t[3 * kTileStride]);
-      red_add_v4(rec + 1, t[4 * kTileStride], t[5 * kTileStride], t[6 * kTileStride], t[7 * kTileStride]);
-      red_add_v4(rec + 2, t[8 * kTileStride], t[9 * kTileStride], t[10 * kTileStride], t[11 * kTileStride]);
-      red_add_v4(rec + 3, t[12 * kTileStride], t[13 * kTileStride], t[14 * kTileStride], 0.f);
+      const int node = m != 0.f ? tile_to_node(tn, bx, by, bz, c) : -1;  // massless nodes are not flushed
+      if (node >= 0) {
+        float4* rec = B.grid + (size_t)node * 4;
+        red_add_v4(rec + 0, m, t[1 * kTileStride], t[2 * kTileStride], t[3 * kTileStride]);
+        red_add_v4(rec + 1, t[4 * kTileStride], t[5 * kTileStride], t[6 * kTileStride], t[7 * kTileStride]);
+        red_add_v4(rec + 2, t[8 * kTileStride], t[9 * kTileStride], t[10 * kTileStride], t[11 * kTileStride]);
+        red_add_v4(rec + 3, t[12 * kTileStride], t[13 * kTileStride], t[14 * kTileStride], 0.f);
+      }
     }
     __syncthreads();
   }
